@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 integral engine: Schwarz-screened direct J/K builds.
+
+One step = one complete J/K build (Coulomb J and exchange K, D in HBM ->
+J, K in HBM) of the selected synthetic workload, through the library's
+CUDA-graph replay of the whole build.  Default workload: cfg4, the
+400-water SCF-like sequence (M = 9600, Schwarz 1e-11), where step k uses
+D_k with D_{k+1} = D_k + 1e-3 C_k C_k^T.
+
+Printed JSON (one line, rank 0):
+  metric/value   ERI quartets/s of the mixed-precision build (surviving
+                 unique contracted shell quartets / build time), all GPUs;
+  jk_builds_per_s, fp64 {...}: builds/s and the plain-FP64 figures;
+  accuracy       |dE| (E = tr(D (J - K/2))), max|dJ|, max|dK| of the mixed
+                 build against the FP64 build on the last density;
+  roofline       dominant ERI kernel: algorithmic FP64 flops (flop model in
+                 origo_tlno_b200/csrc/plan.cpp) per launch / CUDA-event
+                 launch time, against the measured FP64 FMA peak;
+  e2e            the same build through the host-buffer C-ABI call
+                 (H2D of D, D2H of J and K inside the timed region);
+  cpu_baseline   the reference engine (oracle/_ref, compiled from its
+                 sources) or the restatement, timed on a bounded sample.
+`--impl reference` times the reference's CPU J+K on a bounded sample of the
+workload instead and prints the same metric.  Multi-GPU: every rank runs
+an independent replica (the J/K build of one molecule is not sharded), so
+value = sum over ranks and scaling is weak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from origo_tlno_b200 import molecules as MOL  # noqa: E402
+
+METRIC = "ERI quartets/s"
+UNIT = "quartets/s"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _workload(name):
+    if name == "cfg4":
+        mol = MOL.cfg4()
+        return mol, 1e-11, 2000, "cfg4: 400-water cluster, def2-SVP-like basis, M=9600, Schwarz 1e-11"
+    if name == "cfg1":
+        mol = MOL.cfg1()
+        return mol, 1e-12, 45, "cfg1: 24 atoms, M=246, Schwarz 1e-12"
+    if name == "cfg2":
+        mol = MOL.cfg2()
+        return mol, 1e-12, 130, "cfg2: 60 atoms up to f, M=1480, Schwarz 1e-12"
+    if name.startswith("water"):
+        n = int(name[5:])
+        mol = MOL.water_cluster(n, seed=5)
+        return mol, 1e-11, max(1, 5 * n), f"{name}: {n}-water cluster, def2-SVP-like basis, Schwarz 1e-11"
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                        "--format=csv,noheader,nounits", "-lms", "200"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self._p:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._p.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for n, v in zip(names, r[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(self.rows[0][2]) if self.rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _reference_sample(name, seconds_target=15.0):
+    """Times the reference CPU J+K on a bounded sample of the workload.
+    Returns (quartets/s, sample description, kind)."""
+    sys.path.insert(0, ROOT)
+    from origo_tlno_b200 import engine as E
+    from oracle import ref
+    if name in ("cfg4",) or name.startswith("water"):
+        sample_mol = MOL.water_cluster(8, seed=5)
+        tau = 1e-11
+        desc = "8-water sub-cluster of the cfg4 recipe (M=192), Schwarz 1e-11, one J+K build"
+    elif name == "cfg2":
+        sample_mol = MOL.cfg1()
+        tau = 1e-12
+        desc = "cfg1 molecule (M=246) as the bounded sample, one J+K build"
+    else:
+        sample_mol, tau, _, _ = _workload(name)
+        desc = f"{name} whole molecule, one J+K build"
+    D = MOL.random_density(sample_mol.n_sph, max(1, sample_mol.n_sph // 5), seed=77)
+    rb = ref.RefBasis(sample_mol)
+    t = rb.time_jk(D, schwarz=tau, reps=1)
+    secs = float(t[0])
+    return secs, desc, sample_mol, tau
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtlno_ref.so not built"}))
+        return 0
+    # quartet counts of the sample come from the same screening rule; they are
+    # computed with the GPU plan when a device exists, else by the restated
+    # count below.
+    times = []
+    desc = None
+    q = None
+    for i in range(args.warmup + args.steps):
+        secs, desc, mol, tau = _reference_sample(args.config)
+        if q is None:
+            q = _count_quartets(mol, tau)
+        if i >= args.warmup:
+            times.append(secs)
+    t = float(np.median(times))
+    v = q / t
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": args.config, "sample": desc},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def _count_quartets(mol, tau):
+    """Unique contracted shell quartets with Q_ab Q_cd >= tau, from the
+    reference's own Schwarz bounds (oracle/_ref)."""
+    from oracle import ref
+    rb = ref.RefBasis(mol)
+    Q = rb.schwarz()
+    Q = np.sort(Q)[::-1]
+    # pairs (p >= q) with Q_p Q_q >= tau
+    total = 0
+    n = len(Q)
+    for i in range(n):
+        lo, hi = 0, i + 1
+        # count j <= i with Q[j] * Q[i] >= tau (Q sorted descending, j < i has larger Q)
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if Q[i] * Q[mid] >= tau:
+                lo = mid + 1
+            else:
+                hi = mid
+        total += lo
+    return total
+
+
+def run_native(args):
+    import torch
+    from origo_tlno_b200 import engine as E
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mol, tau, n_occ, wdesc = _workload(args.config)
+    M = mol.n_sph
+    ctx = E.Context(mol, device=local).plan(E.ScreeningOptions(integral_threshold=tau,
+                                                               mixed_threshold=args.mixed_threshold))
+    prof = ctx.profile()
+    quartets = prof["quartets"]
+
+    # SCF-like density sequence on the device: D_{k+1} = D_k + 1e-3 C_k C_k^T.
+    nd = args.warmup + args.steps
+    g = torch.Generator(device="cpu").manual_seed(1000)
+    C0 = (torch.randn(M, n_occ, generator=g, dtype=torch.float64) / np.sqrt(M)).to(dev)
+    Ds = [C0 @ C0.T]
+    for k in range(1, nd):
+        Ck = (torch.randn(M, n_occ, generator=g, dtype=torch.float64) / np.sqrt(M)).to(dev)
+        Ds.append(Ds[-1] + 1e-3 * (Ck @ Ck.T))
+    for D in Ds:
+        D.copy_(0.5 * (D + D.T))
+    d_in = torch.empty(M, M, dtype=torch.float64, device=dev)
+    J = torch.empty(M, M, dtype=torch.float64, device=dev)
+    K = torch.empty(M, M, dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+
+    def timed_sequence(mixed):
+        ctx.graph_capture(d_in.data_ptr(), J.data_ptr(), K.data_ptr(), mixed=mixed)
+        torch.cuda.synchronize()
+        ev = []
+        with torch.cuda.stream(stream):
+            for k in range(nd):
+                d_in.copy_(Ds[k])
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.graph_launch()
+                e1.record(stream)
+                ev.append((e0, e1))
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in ev[args.warmup:]]
+        return ms
+
+    # FP64 sequence first (also the accuracy reference for the last density)
+    ms64 = timed_sequence(False)
+    J64, K64 = J.clone(), K.clone()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    with sampler:
+        t_wall0 = time.time()
+        msmx = timed_sequence(True)
+        t_wall = time.time() - t_wall0
+    Dl = Ds[-1]
+    dE = float(torch.sum(Dl * ((J - 0.5 * K) - (J64 - 0.5 * K64))).item())
+    dJ = float((J - J64).abs().max().item())
+    dK = float((K - K64).abs().max().item())
+    t64 = float(np.sum(ms64)) / 1e3
+    tmx = float(np.sum(msmx)) / 1e3
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t64, tmx], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t64, tmx = float(tt[0]), float(tt[1])
+    steps = args.steps
+    value = ws * quartets * steps / tmx
+    value64 = ws * quartets * steps / t64
+
+    # end to end: host D (pinned) -> C-ABI host call -> host J, K
+    Dh = Ds[-1].cpu().numpy()
+    e2e_times = []
+    for r in range(max(2, min(3, args.steps))):
+        t0 = time.time()
+        out = ctx.jk(Dh, want=("J", "K"), mixed=True, validate=False)
+        e2e_times.append(time.time() - t0)
+    e2e_t = float(np.median(e2e_times[1:] if len(e2e_times) > 1 else e2e_times))
+    e2e = {"value": ws * quartets / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(Dh.nbytes),
+           "d2h_bytes_per_step": int(out["J"].nbytes + out["K"].nbytes)}
+
+    # roofline of the dominant kernel (class combination with the largest time)
+    combos = ctx.combos()
+    timings = []
+    for i, cb in enumerate(combos):
+        if cb["n_tiles"] == 0:
+            continue
+        t = ctx.time_combo(i, fp32=False, reps=2)
+        timings.append((t, i, cb))
+    timings.sort(key=lambda x: -x[0])
+    tdom, idom, cdom = timings[0]
+    peak = E.fma_peak_tflops(False, device=local)
+    achieved = cdom["flops"] / (tdom * 1e-3) / 1e12
+    launches_fp64 = sum(1 for cb in combos if cb["n_tiles"] > 0) + 4
+    launches = 2 * sum(1 for cb in combos if cb["n_tiles"] > 0) + 5
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            secs, desc, smol, stau = _reference_sample(args.config)
+            q = _count_quartets(smol, stau)
+            cpu = {"value": q / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": desc + f" ({q} quartets, {secs:.2f} s)"}
+        except Exception as e:  # the reference oracle may be absent
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    clocks = sampler.summary()
+    res = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * tmx / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+f32 mixed (FP64 accumulation)", "data": "synthetic",
+        "config": {"workload": args.config, "description": wdesc, "M": M, "quartets_per_build": quartets,
+                   "primitive_quartets_per_build": prof["primitive_quartets"],
+                   "flops_per_build_model": prof["flops"], "parallelism": f"replicas{ws}",
+                   "l2": "inputs larger than L2 (D, J, K are M*M*8 bytes each)" if M * M * 8 > 126e6 else
+                         "inputs smaller than L2",
+                   "mixed_threshold": args.mixed_threshold, "schwarz": tau},
+        "jk_builds_per_s": ws * steps / tmx,
+        "fp64": {"value": value64, "unit": UNIT, "jk_builds_per_s": ws * steps / t64,
+                 "ms_per_step": 1e3 * t64 / steps},
+        "mixed_speedup_vs_fp64": t64 / tmx,
+        "accuracy": {"abs_dE_Eh": abs(dE), "max_abs_dJ": dJ, "max_abs_dK": dK},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak else None, "traffic": None,
+                     "kernel": f"eri class ({cdom['la']}{cdom['lb']}|{cdom['lc']}{cdom['ld']}) "
+                               f"{'thread-per-quartet' if cdom['fast'] else 'warp-per-quartet'}",
+                     "peak_source": "measured DFMA-chain probe (tlno_gpu_fma_peak) on this GPU"},
+        "e2e": e2e, "gpu_launches": launches * steps,
+        "clocks": clocks, "wall_s_timed": t_wall,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(res))
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--config", default="cfg4")
+    ap.add_argument("--mixed-threshold", type=float, default=1e-9)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_native(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

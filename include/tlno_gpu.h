@@ -1,0 +1,213 @@
+/*
+ * tlno_gpu.h -- C ABI of the B200 (sm_100a) integral engine.
+ *
+ * Drop-in boundary for the origo-tlno integral hot path.  Every entry point
+ * replaces one C++ engine entry of the reference (cited per function, paths
+ * relative to the reference repository) and keeps its argument meaning and
+ * error contract: the reference throws std::runtime_error with an
+ * "eri_ao_tensor_hgp:" prefix; here the same condition returns a negative
+ * status and tlno_gpu_last_error() returns the same message text.
+ *
+ * Conventions
+ *   - Status: 0 = success, < 0 = failure (TLNO_GPU_E_*).
+ *   - Matrices are M x M row-major doubles over spherical AOs, shell by
+ *     shell in input order, 2L+1 functions per shell in PySCF order
+ *     (p: x, y, z; l >= 2: m = -l..l), the reference's AO order
+ *     (integrals/one_electron/onee_matrices.cpp:459-484,
+ *      integrals/two_electron/rys/rys_engine.ipp:2362-2383).
+ *   - Buffers are host memory unless the call takes TLNO_GPU_DEVICE_PTRS,
+ *     in which case every matrix pointer is CUDA device memory of the
+ *     context's device.
+ *   - One context = one basis, one CUDA device, one stream; a context is not
+ *     thread-safe.  There is no CPU fallback: without a usable CUDA device
+ *     every compute call fails with TLNO_GPU_E_CUDA.
+ */
+#ifndef TLNO_GPU_H
+#define TLNO_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TLNO_GPU_OK 0
+#define TLNO_GPU_E_INVALID (-1)   /* invalid argument or input data        */
+#define TLNO_GPU_E_CUDA (-2)      /* CUDA runtime error or no device       */
+#define TLNO_GPU_E_STATE (-3)     /* call out of order (e.g. no plan yet)  */
+#define TLNO_GPU_E_DEVICE (-4)    /* device-side status word reported fault */
+
+/* flags */
+#define TLNO_GPU_DEVICE_PTRS 0x1  /* matrix pointers are device memory       */
+#define TLNO_GPU_WANT_J 0x2
+#define TLNO_GPU_WANT_K 0x4
+#define TLNO_GPU_WANT_G 0x8       /* G = J - K/2 (needs J and K internally)  */
+#define TLNO_GPU_MIXED 0x10       /* mixed FP32/FP64 evaluation              */
+#define TLNO_GPU_NO_VALIDATE 0x20 /* skip the density validation pass        */
+
+typedef struct tlno_gpu_context tlno_gpu_context;
+
+/* Screening options; field meaning of the reference's
+ * fock::ScreeningOptions (integrals/two_electron/fock/jk_direct.hpp:18-24)
+ * plus the mixed-precision split threshold. */
+typedef struct {
+    double integral_threshold;             /* Schwarz: keep Q_ab Q_cd >= tau */
+    double primitive_fastschwarz_threshold; /* accepted; must be 0 (not used) */
+    double decay_threshold;                 /* accepted; must be 0 (not used) */
+    double density_threshold;               /* accepted; must be 0 (not used) */
+    double mixed_threshold;                 /* FP32 when Q_ab Q_cd max|D| < this */
+} tlno_gpu_screening;
+
+/* Plan statistics (the reference's EriPackedPlanProfile counterpart,
+ * integrals/two_electron/twoe_integrals.hpp:166-187). */
+typedef struct {
+    int M;
+    int n_shells;
+    long long shell_pairs;          /* all canonical shell pairs            */
+    long long kept_pairs;           /* pairs that can pass the Schwarz gate */
+    long long quartets;             /* surviving unique contracted quartets */
+    long long primitive_quartets;   /* surviving primitive quartets         */
+    double flops;                   /* algorithmic flop model per J/K build */
+    int n_class_launches;
+} tlno_gpu_profile;
+
+/* Last error message of the calling thread (empty string if none). */
+const char* tlno_gpu_last_error(void);
+/* ABI version (major * 10000 + minor * 100 + patch). */
+int tlno_gpu_version(void);
+/* Number of CUDA devices visible (0 when none). */
+int tlno_gpu_device_count(int* count);
+
+/* Create a context from contracted shells with RAW contraction coefficients;
+ * every Cartesian component is normalised as the reference's make_shell does
+ * (core/shell/shell_contract.cpp:41-48, core/basis/cartesian_shells.hpp:61-74).
+ * centers: 3 per shell (bohr); L: 0..4; nprim: >= 1; exps/coefs: packed per
+ * shell.  Z / atom_xyz: nuclear charges and centres for the attraction
+ * integrals.  Replaces the std::vector<Shell> construction that feeds
+ * build_one_electron_plan (onee_matrices.hpp:41) and build_direct_plan
+ * (jk_direct.hpp:46). */
+int tlno_gpu_create(int n_shells, const double* centers, const int* L, const int* nprim,
+                    const double* exps, const double* coefs, int natom, const int* Z,
+                    const double* atom_xyz, int device, tlno_gpu_context** out);
+
+/* Create a context from per-Cartesian-component records that are already
+ * normalised -- the reference's std::vector<core::basis::Shell> layout
+ * (core/basis/types.hpp:30-35): centers 3 per component, ang 3 per
+ * component, nprim per component, exps/coefs packed.  Components are grouped
+ * into shells as the reference groups them (rys_engine.ipp:1928-2060). */
+int tlno_gpu_create_from_components(int n_components, const double* centers, const int* ang,
+                                    const int* nprim, const double* exps, const double* coefs,
+                                    int natom, const int* Z, const double* atom_xyz, int device,
+                                    tlno_gpu_context** out);
+
+void tlno_gpu_destroy(tlno_gpu_context* ctx);
+
+/* Spherical AO count M and shell count. */
+int tlno_gpu_n_sph(const tlno_gpu_context* ctx);
+int tlno_gpu_n_shells(const tlno_gpu_context* ctx);
+
+/* Build the two-electron plan: Schwarz bounds on the device, class-sorted
+ * screened pairs, quartet schedules.  Replaces fock::build_direct_plan
+ * (integrals/two_electron/fock/jk_direct.hpp:46-48) and
+ * build_eri_packed_plan_for_G_rys (twoe_integrals.hpp:202-204). */
+int tlno_gpu_plan(tlno_gpu_context* ctx, const tlno_gpu_screening* options);
+int tlno_gpu_plan_profile(const tlno_gpu_context* ctx, tlno_gpu_profile* out);
+
+/* Coulomb / exchange build for a real symmetric density D (M x M).
+ * flags: TLNO_GPU_WANT_J / _K / _G select outputs (null pointers allowed for
+ * unselected ones), TLNO_GPU_MIXED selects the mixed-precision path,
+ * TLNO_GPU_DEVICE_PTRS device-resident buffers.  Replaces
+ * fock::build_coulomb_j, fock::build_exchange_k and fock::build_rhf_g
+ * (integrals/two_electron/fock/jk_direct.hpp:82-96): J[a,b] = sum_cd
+ * (ab|cd) D[c,d], K[a,c] = sum_bd (ab|cd) D[b,d], G = J - K/2. */
+int tlno_gpu_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, double* G,
+                int flags);
+
+/* One-electron S, T, V (spherical, M x M).  screening != 0 applies the
+ * reference's default screening (group-pair decay 1e-15, nuclear primitive
+ * 1e-15 / sum|Z|); 0 disables it.  Replaces
+ * evaluate_one_electron_matrices_sph_into / build_one_electron_spherical_matrices
+ * (integrals/one_electron/onee_matrices.hpp:50, 63-66). */
+int tlno_gpu_onee(tlno_gpu_context* ctx, double* S, double* T, double* V, int screening, int flags);
+/* Screening knobs (onee_matrices.hpp:78-79, onee_integrals.hpp:187-188). */
+int tlno_gpu_set_onee_thresholds(tlno_gpu_context* ctx, double group_pair_decay_eps,
+                                 double nuclear_screen_eps);
+
+/* Contracted spherical ERI blocks (A B | C D) for n quartets of shell
+ * indices (4 per quartet); block q is written at out + offsets[q] with layout
+ * [(2La+1)(2Lb+1)] x [(2Lc+1)(2Ld+1)] row-major.  Host buffers.  The
+ * per-quartet producer of the reference is compute_quartet_block_rys_impl
+ * followed by the final pair projector (rys_engine.ipp:13754, 1844). */
+int tlno_gpu_eri_blocks(tlno_gpu_context* ctx, int n_quartets, const int* shells4,
+                        const long long* offsets, double* out);
+
+/* Schwarz bound per canonical shell pair i*(i+1)/2 + j (i >= j), as
+ * get_rys_spherical_pair_schwarz_bounds().pair_group_max
+ * (rys_engine.ipp:16165-16258).  Requires a plan.  Host buffer. */
+int tlno_gpu_schwarz(const tlno_gpu_context* ctx, double* out);
+
+/* Device Boys function F_0..F_maxn at n points (host buffers; out is
+ * n x (maxn+1)).  Reference: core/math/general_math.hpp:6-22. */
+int tlno_gpu_boys(int device, int n, int maxn, const double* x, double* out);
+/* Device Rys roots (t^2) and weights for nroots at n arguments (host
+ * buffers, n x nroots each); fp32 selects the single-precision tables.
+ * Reference: rys_roots_weights (rys_engine.ipp:3823-3838). */
+int tlno_gpu_rys(int device, int n, int nroots, const double* T, double* roots, double* weights,
+                 int fp32);
+
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA)
+ * from a dependent-chain DFMA kernel filling every SM; the roofline
+ * denominator of the FP64 ERI kernels.  fp32 != 0 measures FFMA instead. */
+int tlno_gpu_fma_peak(int device, int fp32, double* tflops);
+
+/* CUDA graph of one J/K build on device buffers (TLNO_GPU_DEVICE_PTRS is
+ * implied): capture once, replay per SCF step after updating D in place. */
+int tlno_gpu_jk_graph_capture(tlno_gpu_context* ctx, const double* d_density, double* d_J,
+                              double* d_K, int flags);
+int tlno_gpu_jk_graph_launch(tlno_gpu_context* ctx);
+/* Waits for the context's stream. */
+int tlno_gpu_synchronize(tlno_gpu_context* ctx);
+/* Raw CUDA stream of the context (cudaStream_t) for event timing. */
+void* tlno_gpu_stream(tlno_gpu_context* ctx);
+
+/* Batched J/K over many molecules in one work queue per class (the
+ * reference has no batch API; its per-molecule equivalent is repeated
+ * build_coulomb_j / build_exchange_k calls).  The batch context owns the
+ * merged plan; densities, J and K are stacked M_m x M_m blocks in molecule
+ * order (offsets returned by tlno_gpu_batch_offsets). */
+typedef struct tlno_gpu_batch tlno_gpu_batch;
+int tlno_gpu_batch_create(int n_mol, tlno_gpu_context* const* ctxs, const tlno_gpu_screening* options,
+                          tlno_gpu_batch** out);
+void tlno_gpu_batch_destroy(tlno_gpu_batch* b);
+long long tlno_gpu_batch_total_elements(const tlno_gpu_batch* b);
+int tlno_gpu_batch_offsets(const tlno_gpu_batch* b, long long* offsets);
+int tlno_gpu_batch_profile(const tlno_gpu_batch* b, tlno_gpu_profile* out);
+int tlno_gpu_batch_jk(tlno_gpu_batch* b, const double* density, double* J, double* K, int flags);
+int tlno_gpu_batch_graph_capture(tlno_gpu_batch* b, const double* d_density, double* d_J, double* d_K,
+                                 int flags);
+int tlno_gpu_batch_graph_launch(tlno_gpu_batch* b);
+int tlno_gpu_batch_synchronize(tlno_gpu_batch* b);
+void* tlno_gpu_batch_stream(tlno_gpu_batch* b);
+
+/* Tuning of the kernel schedule (autotuner output): thread-per-quartet CTA
+ * bra pairs, generic-kernel ket tile, generic warps per CTA, persistent
+ * grid multiplier, and a per-class-combination generic override. */
+typedef struct {
+    int fast_bb;
+    int generic_bk;
+    int generic_warps;
+    int grid_mult;
+} tlno_gpu_tuning;
+int tlno_gpu_set_tuning(tlno_gpu_context* ctx, const tlno_gpu_tuning* t);
+int tlno_gpu_set_combo_generic(tlno_gpu_context* ctx, int combo_id, int force_generic);
+/* Per class-combination statistics of the current plan: for i < n, writes
+ * (X, Y, la, lb, lc, ld, fast, n_tiles) into ints[8*i] and
+ * (quartets, prim_quartets, flops) into dbl[3*i]; returns the count. */
+int tlno_gpu_plan_combos(const tlno_gpu_context* ctx, int max_n, int* ints, double* dbl);
+/* Time one class combination alone (ms per launch, CUDA events) for the
+ * autotuner; runs on the context's stream with its device buffers. */
+int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int fp32, int reps, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TLNO_GPU_H */

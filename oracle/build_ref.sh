@@ -1,0 +1,53 @@
+#!/usr/bin/env bash
+# TEST INFRASTRUCTURE: compiles the UNMODIFIED origo-tlno reference engine
+# from its own sources (read in place under /root/reference, never copied)
+# together with oracle/ref_harness.cpp into oracle/_ref/libtlno_ref.so.
+#
+# The reference's CMake build is not used; this recipe compiles the few
+# translation units of the integral hot path directly with g++, with the
+# reference's AVX2 "Release" options (CMakeLists.txt:9-34: -march=x86-64-v3,
+# -O3 -DNDEBUG, OpenMP, C++17).  Output goes only to oracle/_ref/.
+#
+# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+set -euo pipefail
+HERE="$(cd "$(dirname "$0")" && pwd)"
+REF="${1:-/root/reference}"
+OUT="$HERE/_ref"
+OBJ="$OUT/obj"
+# The image may export CXX pointing at a compiler without libgomp; the
+# reference build needs OpenMP, so use the system g++ unless REF_CXX is set.
+CXX="${REF_CXX:-/usr/bin/g++}"
+if [ ! -d "$REF/integrals" ]; then
+    echo "build_ref: reference sources not found at $REF" >&2
+    exit 2
+fi
+mkdir -p "$OBJ"
+FLAGS=(-std=c++17 -O3 -DNDEBUG -march=x86-64-v3 -mtune=generic -fopenmp -fPIC -I"$REF" -w)
+SRCS=(
+  core/shell/shell_math.cpp
+  core/shell/shell_contract.cpp
+  core/shell/cart2sph.cpp
+  core/math/general_math.cpp
+  integrals/one_electron/onee_integrals.cpp
+  integrals/one_electron/onee_matrices.cpp
+  integrals/two_electron/fock/jk_direct.cpp
+)
+pids=()
+objs=()
+for s in "${SRCS[@]}"; do
+  o="$OBJ/$(echo "$s" | tr '/' '_' ).o"
+  objs+=("$o")
+  if [ ! -f "$o" ] || [ "$REF/$s" -nt "$o" ]; then
+    "$CXX" "${FLAGS[@]}" -c "$REF/$s" -o "$o" &
+    pids+=($!)
+  fi
+done
+H="$OBJ/ref_harness.o"
+objs+=("$H")
+if [ ! -f "$H" ] || [ "$HERE/ref_harness.cpp" -nt "$H" ]; then
+  "$CXX" "${FLAGS[@]}" -c "$HERE/ref_harness.cpp" -o "$H" &
+  pids+=($!)
+fi
+for p in "${pids[@]}"; do wait "$p"; done
+"$CXX" -shared -fopenmp -o "$OUT/libtlno_ref.so" "${objs[@]}"
+echo "build_ref: wrote $OUT/libtlno_ref.so"

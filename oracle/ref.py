@@ -1,0 +1,169 @@
+"""TEST INFRASTRUCTURE: ctypes wrapper of oracle/_ref/libtlno_ref.so, the
+UNMODIFIED origo-tlno reference engine compiled from its own sources by
+oracle/build_ref.sh together with oracle/ref_harness.cpp.
+
+Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline and the
+`--impl reference` arm) may use this module, as the checker or as the timed
+CPU baseline -- never as the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_ref", "libtlno_ref.so")
+
+_lib = None
+_gomp = None
+
+
+def _omp():
+    """libgomp as loaded by the reference library (OpenMP thread control:
+    the reference's G and K endpoints refuse more than one thread,
+    rys_engine.ipp:16853-16857)."""
+    global _gomp
+    if _gomp is None:
+        lib()
+        _gomp = C.CDLL("libgomp.so.1")
+        _gomp.omp_get_max_threads.restype = C.c_int
+        _gomp.omp_set_num_threads.argtypes = [C.c_int]
+    return _gomp
+
+
+class single_thread:
+    def __enter__(self):
+        self.prev = _omp().omp_get_max_threads()
+        _omp().omp_set_num_threads(1)
+
+    def __exit__(self, *a):
+        _omp().omp_set_num_threads(self.prev)
+
+
+def set_threads(n: int) -> None:
+    _omp().omp_set_num_threads(int(n))
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise FileNotFoundError(f"{LIB_PATH} not built (oracle/build_ref.sh)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_basis_create.restype = vp
+        L.ref_basis_create.argtypes = [C.c_int, vp, vp, vp, vp, vp, C.c_int, vp, vp]
+        L.ref_basis_destroy.argtypes = [vp]
+        L.ref_basis_n_sph.argtypes = [vp]
+        L.ref_basis_n_cart.argtypes = [vp]
+        L.ref_basis_component_coefs.argtypes = [vp, C.c_int, vp]
+        L.ref_onee_sph.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.ref_onee_cart.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.ref_jk.argtypes = [vp, vp, C.c_double, C.c_double, vp, vp, vp]
+        L.ref_time_jk.argtypes = [vp, vp, C.c_double, C.c_int, vp]
+        L.ref_eri_sph_block.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]
+        L.ref_schwarz_pair_max.argtypes = [vp, vp]
+        L.ref_boys_single.restype = C.c_double
+        L.ref_boys_single.argtypes = [C.c_int, C.c_double]
+        L.ref_boys_r000_all.argtypes = [C.c_int, C.c_double, C.c_double, vp]
+        L.ref_boys_hgp.restype = C.c_double
+        L.ref_boys_hgp.argtypes = [C.c_int, C.c_double]
+        L.ref_rys_roots.argtypes = [C.c_int, C.c_double, vp, vp]
+        L.ref_rys_roots_accurate.argtypes = [C.c_int, C.c_double, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _chk(rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + lib().ref_last_error().decode())
+
+
+class RefBasis:
+    def __init__(self, mol):
+        centers, Ls, nprim, exps, coefs = mol.soa()
+        self._keep = [np.ascontiguousarray(centers, dtype=np.float64), np.ascontiguousarray(Ls, dtype=np.int32),
+                      np.ascontiguousarray(nprim, dtype=np.int32), np.ascontiguousarray(exps, dtype=np.float64),
+                      np.ascontiguousarray(coefs, dtype=np.float64), np.ascontiguousarray(mol.charges, dtype=np.int32),
+                      np.ascontiguousarray(mol.coords, dtype=np.float64)]
+        c, l, n, e, k, z, x = self._keep
+        self.h = lib().ref_basis_create(len(mol.shells), c.ctypes.data, l.ctypes.data, n.ctypes.data,
+                                        e.ctypes.data, k.ctypes.data, len(z), z.ctypes.data, x.ctypes.data)
+        if not self.h:
+            raise RuntimeError("reference: " + lib().ref_last_error().decode())
+        self.M = lib().ref_basis_n_sph(self.h)
+        self.n_cart = lib().ref_basis_n_cart(self.h)
+        self.mol = mol
+
+    def close(self):
+        if self.h:
+            lib().ref_basis_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def onee(self, screening=True):
+        M = self.M
+        S, T, V = np.empty((M, M)), np.empty((M, M)), np.empty((M, M))
+        _chk(lib().ref_onee_sph(self.h, 1 if screening else 0, S.ctypes.data, T.ctypes.data, V.ctypes.data))
+        return S, T, V
+
+    def jk(self, D, schwarz=1e-12, density_threshold=0.0, want=("J", "K", "G")):
+        M = self.M
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        out = {k: np.empty((M, M)) for k in want}
+        with single_thread():
+            _chk(lib().ref_jk(self.h, D.ctypes.data, schwarz, density_threshold,
+                              out["J"].ctypes.data if "J" in out else None,
+                              out["K"].ctypes.data if "K" in out else None,
+                              out["G"].ctypes.data if "G" in out else None))
+        return out
+
+    def time_jk(self, D, schwarz=1e-12, reps=1):
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        t = np.empty(reps)
+        with single_thread():
+            _chk(lib().ref_time_jk(self.h, D.ctypes.data, schwarz, reps, t.ctypes.data))
+        return t
+
+    def eri_block(self, a, b, c, d):
+        Ls = [s.L for s in self.mol.shells]
+        out = np.empty((2 * Ls[a] + 1) * (2 * Ls[b] + 1) * (2 * Ls[c] + 1) * (2 * Ls[d] + 1))
+        _chk(lib().ref_eri_sph_block(self.h, a, b, c, d, out.ctypes.data))
+        return out.reshape((2 * Ls[a] + 1) * (2 * Ls[b] + 1), (2 * Ls[c] + 1) * (2 * Ls[d] + 1))
+
+    def schwarz(self):
+        ns = len(self.mol.shells)
+        out = np.empty(ns * (ns + 1) // 2)
+        with single_thread():
+            _chk(lib().ref_schwarz_pair_max(self.h, out.ctypes.data))
+        return out
+
+
+def boys_single(n: int, x: float) -> float:
+    return lib().ref_boys_single(n, x)
+
+
+def boys_r000_all(max_n: int, x: float, p: float) -> np.ndarray:
+    out = np.empty(max_n + 1)
+    lib().ref_boys_r000_all(max_n, x, p, out.ctypes.data)
+    return out
+
+
+def rys_roots(n: int, t: float, accurate: bool = False):
+    r = np.empty(n)
+    w = np.empty(n)
+    f = lib().ref_rys_roots_accurate if accurate else lib().ref_rys_roots
+    f(n, t, r.ctypes.data, w.ctypes.data)
+    return r, w

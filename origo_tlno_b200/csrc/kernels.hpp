@@ -1,0 +1,49 @@
+// Host-visible launch wrappers of the device code in kernels.cu.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tlno_gpu {
+namespace dev {
+struct PlanView;
+struct ClassLaunch;
+struct OneeLaunch;
+}  // namespace dev
+
+// Uploads the constant tables (Boys, Rys, Cartesian, cart->sph) for the
+// current device; idempotent per device.
+void ensure_device_tables();
+
+// Shared-memory bytes per warp of the generic kernel for a class.
+int generic_warp_bytes(int la, int lb, int lc, int ld);
+
+void launch_eri_store(const dev::PlanView& pv, const dev::ClassLaunch& cl, cudaStream_t s);
+void launch_eri_schwarz(const dev::PlanView& pv, const dev::ClassLaunch& cl, cudaStream_t s);
+void launch_eri_jk_generic(const dev::PlanView& pv, const dev::ClassLaunch& cl, bool fp32,
+                           int warps, int grid, cudaStream_t s);
+// Thread-per-quartet kernels for the classes that have one; returns false
+// when the class has no specialised kernel.
+bool launch_eri_jk_fast(const dev::PlanView& pv, const dev::ClassLaunch& cl, bool fp32,
+                        int grid, cudaStream_t s);
+bool has_fast_kernel(int la, int lb, int lc, int ld);
+
+void launch_onee(const dev::OneeLaunch& L, cudaStream_t s);
+// out = (X + X^T) / 2 for `count` stacked M x M blocks (offsets per block).
+void launch_symmetrize(double* X, const long long* offsets, const int* dims, int count, int max_m,
+                       cudaStream_t s);
+void launch_symmetrize_single(double* X, int M, cudaStream_t s);
+// *out = max |x_i| over n elements.
+void launch_absmax(const double* x, long long n, double* out, cudaStream_t s);
+// Density contract check: bit 1 = non-finite entry, bit 2 = asymmetric
+// beyond 128 eps * max(1, |Dij|, |Dji|) (direct_build.ipp:25-96).
+void launch_validate_density(const double* D, int M, unsigned int* status, cudaStream_t s);
+// G = J - K / 2 over n elements.
+void launch_combine_g(const double* J, const double* K, double* G, long long n, cudaStream_t s);
+// Dependent-chain FMA throughput probe: returns TFLOP/s.
+double measure_fma_peak(bool fp32);
+void launch_boys_test(const double* x, int n, int maxn, double* out, cudaStream_t s);
+void launch_rys_test(const double* t, int n, int nroots, int fp32, double* roots, double* weights,
+                     cudaStream_t s);
+
+}  // namespace tlno_gpu

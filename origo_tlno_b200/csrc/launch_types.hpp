@@ -1,0 +1,99 @@
+// Plain launch descriptors shared by the host engine and the device code
+// (no device-only constructs, so host C++ translation units can include it).
+#pragma once
+
+namespace tlno_gpu {
+namespace dev {
+
+struct DPrimPair {
+    double p, Px, Py, Pz, w, invp;
+};
+
+// Device view of one plan (or of a batch of plans: every pair carries the
+// AO offset of its molecule, so one launch can serve many molecules).
+struct PlanView {
+    const double* shell_xyz;      // 3 per shell
+    const int* shell_L;
+    const int* shell_sph;         // first spherical AO of the shell (molecule-local)
+    const int* pair_A;            // oriented shells, L_A >= L_B
+    const int* pair_B;
+    const int* pair_prim_off;
+    const int* pair_nprim;
+    const double* pair_Q;         // Schwarz bound
+    const int* pair_mol;          // molecule of the pair (batch), may be null
+    const DPrimPair* prim;
+    // Per-molecule matrix bases (batch): density/J/K at base + M*M offsets.
+    const long long* mol_mat_off; // element offset of the molecule's M x M block
+    const int* mol_M;
+};
+
+// One bra block of a quartet-class schedule: up to `nbra` consecutive bra
+// pairs (sorted by Schwarz bound) against the ket list of the same molecule.
+struct BlockDesc {
+    int bra0;      // first bra pair (global sorted index)
+    int nbra;      // bras in this block
+    int ket0;      // first pair of the ket class list of this molecule
+    int nket;      // length of that list
+    int ilocal0;   // position of bra0 inside its own class list (triangle test)
+    int pad;
+};
+
+// Quartet class and the schedule of one launch.
+struct ClassLaunch {
+    int la, lb, lc, ld;
+    int same;                     // bra class == ket class (triangle j <= i)
+    int bb, bk;                   // tile shape: bra pairs x ket pairs
+    const BlockDesc* blocks;
+    const int* tile_prefix;       // per block: first tile index (n_blocks + 1)
+    int n_blocks;
+    int tile_begin, tile_end;     // tile range of this launch
+    double tau;                   // Schwarz threshold
+    // Precision split: mode 0 = every quartet; 1 = quartets with
+    // Q_ab Q_cd max|D| >= tau_mix only (FP64 part); 2 = the complement.
+    int prec_mode;
+    double tau_mix;
+    const double* dmax;           // device scalar max|D| (per build)
+    // Explicit quartet list (STORE / SCHWARZ modes): pair indices.
+    const int* q_bra;
+    const int* q_ket;
+    int n_quartets;
+    // Outputs.
+    double* out;                  // STORE: blocks; SCHWARZ: Q per quartet
+    const long long* out_off;     // STORE: element offset per quartet
+    const double* dens;
+    double* J;
+    double* K;
+    int M;                        // single-molecule AO count (when no batch)
+    int want_j, want_k;
+    unsigned int* status;         // device error word (0 = ok)
+};
+
+struct OneePair {
+    int A, B;         // oriented shells, L_A >= L_B
+    int do_st, do_v;
+};
+
+struct OneeLaunch {
+    const double* shell_xyz;
+    const int* shell_L;
+    const int* shell_nprim;
+    const int* shell_prim;
+    const int* shell_sph;
+    const double* exps;
+    const double* c_radial;
+    const double* maxc;        // per primitive: max |normalised coefficient| over the group
+    const double* comp_coef;   // normalised coefficient per Cartesian component and primitive
+    const int* comp_off;       // per shell: offset into comp_coef
+    const OneePair* pairs;
+    int n_pairs;
+    const double* nuc;         // 4 per nucleus: x, y, z, Z (zero-charge nuclei removed)
+    int n_nuc;
+    double screen_thr;         // eps / sum|Z| (0 disables)
+    int M;
+    double* S;
+    double* T;
+    double* V;
+};
+
+}  // namespace dev
+}  // namespace tlno_gpu

@@ -1,0 +1,93 @@
+// Two-electron plan: Schwarz-screened shell pairs sorted by (La, Lb) class
+// and bound, device-resident pair/primitive data and the quartet-class
+// schedules; one-electron pair list.
+#pragma once
+
+#include <array>
+#include <vector>
+
+#include "engine.hpp"
+#include "launch_types.hpp"
+
+namespace tlno_gpu {
+
+struct Tuning {
+    int fast_bb = 4;        // bra pairs per CTA (warps) of the thread-per-quartet kernels
+    int generic_bk = 16;    // ket pairs per tile of the warp-per-quartet kernel
+    int generic_warps = 0;  // 0 = from shared-memory budget
+    int grid_mult = 8;      // CTAs per SM for persistent launches
+    std::array<int, 256> force_generic{};  // per class combo: 1 = never use the fast kernel
+};
+
+struct ComboSchedule {
+    int X = 0, Y = 0;            // pair classes, X >= Y
+    int la = 0, lb = 0, lc = 0, ld = 0;
+    bool fast = false;
+    int bb = 1, bk = 16;
+    std::vector<dev::BlockDesc> blocks;
+    std::vector<int> prefix;
+    DeviceBuffer d_blocks, d_prefix;
+    int n_tiles = 0;
+    long long quartets = 0;       // surviving contracted quartets
+    long long prim_quartets = 0;  // surviving primitive quartets
+    double flops = 0.0;           // algorithmic flop model
+};
+
+// Pair data of one molecule (host), before merging into a device plan.
+struct MolPairs {
+    std::vector<int> A, B, nprim, cls;
+    std::vector<double> Q;          // sorted order
+    std::array<int, kMaxPairClasses> cls_begin{}, cls_count{};
+    std::vector<double> Q_canonical;  // per canonical pair i*(i+1)/2+j
+    double Qmax = 0.0;
+};
+
+class Plan2e {
+public:
+    // Device plan over one or more molecules (batch).
+    double tau = 1e-12;
+    int n_mol = 0;
+    std::vector<int> mol_shell_off;   // global shell offset per molecule
+    std::vector<int> mol_M;
+    std::vector<long long> mol_mat_off;
+    std::vector<MolPairs> mol_pairs;
+    // Global sorted pair arrays (molecule-major, class, Q descending).
+    std::vector<int> pair_A, pair_B, pair_nprim, pair_prim_off, pair_mol;
+    std::vector<double> pair_Q;
+    std::vector<ComboSchedule> combos;
+    DeviceBuffer d_shell_xyz, d_shell_L, d_shell_sph;
+    DeviceBuffer d_pair_A, d_pair_B, d_pair_prim_off, d_pair_nprim, d_pair_Q, d_pair_mol;
+    DeviceBuffer d_prim, d_mol_mat_off, d_mol_M;
+    long long total_quartets = 0, total_prim_quartets = 0;
+    double total_flops = 0.0;
+    long long total_pairs = 0, kept_pairs = 0;
+
+    dev::PlanView view() const;
+};
+
+// Computes Schwarz bounds of every pair of a basis on the device and returns
+// the sorted, screened pair list of that molecule.
+MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s);
+
+// Builds the device plan for a set of bases (one per molecule) with their
+// already screened pair lists.
+void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vector<MolPairs>&& pairs,
+                double tau, const Tuning& tune, cudaStream_t s);
+
+// Primitive pair records of shells (A, B) with the reference's skip of zero
+// coefficient products (rys_engine.ipp:2244-2279).
+void primitive_pairs(const Basis& b, int A, int B, std::vector<dev::DPrimPair>& out);
+int primitive_pair_count(const Basis& b, int A, int B);
+
+// One-electron plan: kept shell pairs with the reference's group-pair decay
+// screening (onee_matrices.cpp:96-216).
+struct OneePlan {
+    std::vector<dev::OneePair> pairs;
+    std::vector<double> maxc;  // per primitive
+    std::vector<double> nuc;   // x, y, z, Z of nonzero-charge nuclei
+    double screen_thr = 0.0;
+    DeviceBuffer d_pairs, d_maxc, d_nuc;
+};
+void build_onee_plan(OneePlan& p, const Basis& b, double decay_eps, double nuclear_eps);
+
+}  // namespace tlno_gpu

@@ -1,0 +1,44 @@
+// Host-side generation of the interpolation tables the device kernels read:
+// the Boys function F_n(x) on a 0.01 grid and the Rys roots/weights per root
+// count on the same grid, plus the large-T Hermite asymptotic constants.
+#pragma once
+
+#include <vector>
+
+namespace tlno_gpu {
+
+// Boys table: F_n(k * kBoysDx) for k = 0..kBoysRows-1 and n = 0..kBoysOrders-1,
+// stored grid-major (row k holds all orders contiguously) so that one Taylor
+// evaluation reads a single contiguous run.
+constexpr int kBoysOrders = 40;       // orders 0..39 (Taylor needs n+5)
+constexpr int kBoysGrid = 4000;       // x in [0, 40]
+constexpr int kBoysRows = kBoysGrid + 8;
+constexpr double kBoysDx = 0.01;
+constexpr double kBoysXMax = 40.0;
+
+// Rys tables: root counts 1..kRysMaxN, grid T = k * 0.01 for
+// k = 0 .. rows(N)-1 with rows(N) = int(tmax(N) * 100) + 7, layout
+// [k * N + n] for roots (t^2) and weights separately.
+constexpr int kRysMaxN = 9;
+constexpr double kRysDx = 0.01;
+
+struct HostTables {
+    std::vector<double> boys;                 // kBoysRows * kBoysOrders
+    double rys_tmax[kRysMaxN + 1] = {0};
+    int rys_rows[kRysMaxN + 1] = {0};
+    std::vector<double> rys_roots[kRysMaxN + 1];
+    std::vector<double> rys_weights[kRysMaxN + 1];
+    // Positive Gauss-Hermite nodes squared and weights for 2N-point rules.
+    double herm_root2[kRysMaxN + 1][kRysMaxN] = {{0}};
+    double herm_weight[kRysMaxN + 1][kRysMaxN] = {{0}};
+};
+
+// Builds (once per process, thread-safe) and returns the tables.
+const HostTables& host_tables();
+
+// Accurate (non-tabulated) generators, exposed for self-checks.
+void boys_quadrature(int max_n, double x, double* out);
+bool rys_rule_accurate(int n, double t, double* roots, double* weights);
+double rys_tmax(int n);
+
+}  // namespace tlno_gpu
