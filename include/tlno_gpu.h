@@ -203,8 +203,10 @@ int tlno_gpu_set_combo_generic(tlno_gpu_context* ctx, int combo_id, int force_ge
  * (quartets, prim_quartets, flops) into dbl[3*i]; returns the count. */
 int tlno_gpu_plan_combos(const tlno_gpu_context* ctx, int max_n, int* ints, double* dbl);
 /* Time one class combination alone (ms per launch, CUDA events) for the
- * autotuner; runs on the context's stream with its device buffers. */
-int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int fp32, int reps, double* ms);
+ * autotuner; runs on the context's stream with its device buffers.
+ * mode bits: 1 = FP32 evaluation, 2 = skip the J digestion, 4 = skip the K
+ * digestion (2|4 = ERI evaluation only). */
+int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int reps, double* ms);
 
 #ifdef __cplusplus
 }

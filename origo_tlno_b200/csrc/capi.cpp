@@ -18,6 +18,7 @@
 #include "kernels.hpp"
 #include "plan.hpp"
 #include "tables.hpp"
+#include "context.hpp"
 
 using namespace tlno_gpu;
 
@@ -95,9 +96,7 @@ void validate_density_host(const double* D, int M) {
     }
 }
 
-struct JkWork {
-    DeviceBuffer D, J, K, G, dmax, status;
-};
+
 
 // Enqueues one J/K build on stream s over device buffers.
 void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const double* dD, double* dJ,
@@ -155,49 +154,7 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
 
 }  // namespace
 
-struct tlno_gpu_context {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    Basis basis;
-    std::unique_ptr<Plan2e> plan;
-    tlno_gpu_screening screening{1e-12, 0, 0, 0, 1e-9};
-    Tuning tune;
-    OneePlan onee;
-    int onee_state = -1;  // screening flag the 1e plan was built with
-    double onee_decay_eps = 1e-15, onee_nuclear_eps = 1e-15;
-    DeviceBuffer d_shell_xyz, d_shell_L, d_shell_nprim, d_shell_prim, d_shell_sph, d_exps, d_crad;
-    DeviceBuffer d_comp_coef, d_comp_off;
-    JkWork w;
-    DeviceBuffer d_S, d_T, d_V;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-
-    ~tlno_gpu_context() {
-        if (device >= 0) cudaSetDevice(device);
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-struct tlno_gpu_batch {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::vector<Basis> bases;
-    Plan2e plan;
-    tlno_gpu_screening screening{};
-    Tuning tune;
-    JkWork w;
-    long long total = 0;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    ~tlno_gpu_batch() {
-        cudaSetDevice(device);
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        if (graph) cudaGraphDestroy(graph);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
+void tlno_gpu::set_last_error(const std::string& message) { g_error = message; }
 
 namespace {
 
@@ -696,7 +653,8 @@ int tlno_gpu_plan_combos(const tlno_gpu_context* ctx, int max_n, int* ints, doub
     return rc == TLNO_GPU_OK ? count : rc;
 }
 
-int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int fp32, int reps, double* ms) {
+int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int reps, double* ms) {
+    const int fp32 = mode & 1;
     return guarded([&] {
         if (!ctx || !ctx->plan || !ms) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan");
         Plan2e& plan = *ctx->plan;
@@ -722,8 +680,8 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int fp32, int re
         cl.J = ctx->w.J.as<double>();
         cl.K = ctx->w.K.as<double>();
         cl.M = M;
-        cl.want_j = 1;
-        cl.want_k = 1;
+        cl.want_j = (mode & 2) ? 0 : 1;
+        cl.want_k = (mode & 4) ? 0 : 1;
         int sms = 0;
         TLNO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
         const int grid = sms * ctx->tune.grid_mult;

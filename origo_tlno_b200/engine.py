@@ -210,9 +210,11 @@ class Context:
             out.append(d)
         return out
 
-    def time_combo(self, index: int, fp32: bool = False, reps: int = 3) -> float:
+    def time_combo(self, index: int, fp32: bool = False, reps: int = 3, want_j: bool = True,
+                   want_k: bool = True) -> float:
         ms = C.c_double()
-        N.check(N.lib().tlno_gpu_time_combo(self.h, index, 1 if fp32 else 0, reps, C.byref(ms)))
+        mode = (1 if fp32 else 0) | (0 if want_j else 2) | (0 if want_k else 4)
+        N.check(N.lib().tlno_gpu_time_combo(self.h, index, mode, reps, C.byref(ms)))
         return ms.value
 
 
