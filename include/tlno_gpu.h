@@ -139,6 +139,25 @@ int tlno_gpu_set_onee_thresholds(tlno_gpu_context* ctx, double group_pair_decay_
 int tlno_gpu_eri_blocks(tlno_gpu_context* ctx, int n_quartets, const int* shells4,
                         const long long* offsets, double* out);
 
+/* The same ERI blocks as tlno_gpu_eri_blocks, without any device
+ * allocation: no cudaMalloc, cudaFree or allocating library call.  For
+ * callers that cannot allocate device memory -- code that works inside a
+ * device-memory budget owned by another allocator (a framework's pool), on a
+ * latency-critical path where an allocation may synchronise the device, or
+ * that must not grow its device footprint after start-up.  No counterpart
+ * in the reference (its engine is CPU-only).
+ * d_out is caller-owned device memory of the context's device; block q is
+ * written at d_out + offsets[q] (element offsets, host array); shells4 is a
+ * host array.  Per-call scratch (pair tables, primitive pairs, quartet lists)
+ * lives in one fixed 8 MiB device array that every device loading the
+ * library holds until exit; a request needing more fails with
+ * TLNO_GPU_E_INVALID and a message naming the sizes (split it).  The first
+ * call on a device looks up that array's address (cudaGetSymbolAddress), so
+ * it should come before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (e.g. from two host threads) race. */
+int tlno_gpu_eri_blocks_noalloc(tlno_gpu_context* ctx, int n_quartets, const int* shells4,
+                                const long long* offsets, double* d_out);
+
 /* Schwarz bound per canonical shell pair i*(i+1)/2 + j (i >= j), as
  * get_rys_spherical_pair_schwarz_bounds().pair_group_max
  * (rys_engine.ipp:16165-16258).  Requires a plan.  Host buffer. */

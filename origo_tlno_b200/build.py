@@ -22,7 +22,7 @@ CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu"]
 FAST_COUNT = 11  # entries of TLNO_FAST_CLASSES in csrc/fast_classes.hpp
 CPP_SOURCES = ["tables.cpp", "basis.cpp", "plan.cpp", "capi.cpp"]
 
