@@ -23,7 +23,14 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["kernels.cu", "noalloc.cu"]
-FAST_COUNT = 11  # entries of TLNO_FAST_CLASSES in csrc/fast_classes.hpp
+def _fast_count():
+    """Number of compile-time ERI classes (TLNO_FAST_COUNT in csrc/fast_classes.hpp)."""
+    import re
+    text = open(os.path.join(CSRC, "fast_classes.hpp")).read()
+    return int(re.search(r"#define TLNO_FAST_COUNT (\d+)", text).group(1))
+
+
+FAST_COUNT = _fast_count()
 CPP_SOURCES = ["tables.cpp", "basis.cpp", "plan.cpp", "capi.cpp"]
 
 

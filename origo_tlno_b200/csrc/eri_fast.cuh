@@ -1,14 +1,32 @@
-// Thread-per-quartet Rys ERI + J/K kernel for the light angular-momentum
-// classes, with the class fixed at compile time so the 2-D recurrences, the
-// contracted radial accumulators, the horizontal transfer and the spherical
-// projection all live in registers.
+// Compile-time-class Rys ERI + J/K kernel for angular momenta up to d
+// (thread per contracted quartet, the quartet's work sliced over TPQ warps).
 //
-// Tile: one warp per bra shell pair, 32 consecutive ket shell pairs (one per
-// lane), `bb` warps per CTA on consecutive bra pairs; kets are sorted by
-// Schwarz bound so a lane whose quartet fails the bound ends the warp's row.
-// J[ab] is reduced over the warp before its atomic update; the other five
-// digestion targets are updated per lane with FP64 atomics.
+// Tile: a group of TPQ warps takes one bra shell pair and 32 consecutive ket
+// shell pairs of the same class (one quartet per lane); a CTA holds BBQ
+// groups on consecutive bra pairs.  Kets are sorted by Schwarz bound, so the
+// quartets of a tile that fail the bound form a suffix.
+//
+// Phase 1 (registers): every thread of a quartet evaluates the primitive
+// loop (Rys roots/weights, 2-D VRR) and accumulates its own slice of the
+// contracted radial integrals (a0|c0): rows ia = g, g+TPQ, ... of the
+// NAS x NCS block, g = warp index inside the group.  The slice is fixed at
+// compile time, so the accumulators stay in registers; TPQ is the smallest
+// power of two whose slice holds at most kMaxAccPerSlice accumulators.
+// Phase 2: ket HRR and ket spherical projection of the owned rows, written
+// to shared memory as (a0|cd)_sph rows.
+// Phase 3: after a barrier, each warp takes a share of the ket columns
+// (c,d)_sph, applies the bra HRR and projection and digests the finished
+// (ab|cd) column into J and K (J[ab] warp-reduced, the rest FP64 atomics
+// from per-thread partial sums).
+//
+// Arithmetic follows the reference's producer: contracted radial
+// accumulation, contracted-space HRR, final pair projection
+// (rys_engine.ipp:12585-13748, 3141-3362, 1801-1860) and the 8-fold J/K
+// digestion (consumer_policies.ipp:87-221).
 #pragma once
+
+#include <type_traits>
+#include <utility>
 
 #include "eri_common.cuh"
 
@@ -19,29 +37,51 @@ __host__ __device__ constexpr int ce_ncart(int L) { return (L + 1) * (L + 2) / 2
 __host__ __device__ constexpr int ce_nsph(int L) { return 2 * L + 1; }
 __host__ __device__ constexpr int ce_off(int L) { return L * (L + 1) * (L + 2) / 6; }
 __host__ __device__ constexpr int ce_cum(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
-// Cartesian exponents of flat index f (reference order).
+// Cartesian exponents of flat index f (reference order: lx = L..0, then
+// ly = L-lx..0), in closed form so that they fold at compile time.
 __host__ __device__ constexpr int ce_L(int f) {
     int L = 0;
     while (ce_cum(L) <= f) ++L;
     return L;
 }
-__host__ __device__ constexpr int ce_x(int f) {
-    const int L = ce_L(f);
-    int loc = f - ce_off(L);
-    int x = L;
-    while (loc >= L - x + 1) { loc -= L - x + 1; --x; }
-    return x;
+// dx = L - lx: the local index is dx(dx+1)/2 + lz.
+__host__ __device__ constexpr int ce_dx(int f) {
+    const int loc = f - ce_off(ce_L(f));
+    int dx = 0;
+    while ((dx + 1) * (dx + 2) / 2 <= loc) ++dx;
+    return dx;
 }
-__host__ __device__ constexpr int ce_y(int f) {
-    const int L = ce_L(f);
-    int loc = f - ce_off(L);
-    int x = L;
-    while (loc >= L - x + 1) { loc -= L - x + 1; --x; }
-    return L - x - loc;
+__host__ __device__ constexpr int ce_x(int f) { return ce_L(f) - ce_dx(f); }
+__host__ __device__ constexpr int ce_z(int f) {
+    const int dx = ce_dx(f);
+    return f - ce_off(ce_L(f)) - dx * (dx + 1) / 2;
 }
-__host__ __device__ constexpr int ce_z(int f) { return ce_L(f) - ce_x(f) - ce_y(f); }
+__host__ __device__ constexpr int ce_y(int f) { return ce_dx(f) - ce_z(f); }
 __host__ __device__ constexpr int ce_flat(int x, int y, int z) {
     return ce_off(x + y + z) + (y + z) * (y + z + 1) / 2 + z;
+}
+static_assert(ce_x(ce_flat(2, 1, 0)) == 2 && ce_y(ce_flat(2, 1, 0)) == 1 && ce_z(ce_flat(0, 1, 3)) == 3 &&
+                  ce_x(ce_flat(0, 0, 4)) == 0 && ce_z(ce_flat(1, 1, 1)) == 1,
+              "Cartesian index round trip");
+
+// Non-zero pattern of the Cartesian->spherical map (real solid harmonics,
+// order m = -l..l; Cartesians xx, xy, xz, yy, yz, zz for d), so that the
+// projection skips structural zeros at compile time.
+__host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
+    if (L <= 1) return s == c;
+    if (L == 2) {
+        return (s == 0 && c == 1) || (s == 1 && c == 4) || (s == 2 && (c == 0 || c == 3 || c == 5)) ||
+               (s == 3 && c == 2) || (s == 4 && (c == 0 || c == 3));
+    }
+    return true;
+}
+
+constexpr int kMaxAccPerSlice = 48;
+
+__host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
+    int t = 1;
+    while (t < 32 && ((nas + t - 1) / t) * ncs > kMaxAccPerSlice) t *= 2;
+    return t;
 }
 
 template <int LA, int LB, int LC, int LD>
@@ -56,299 +96,373 @@ struct FastShape {
     static constexpr int NCC = ce_ncart(LC), NCD = ce_ncart(LD);
     static constexpr int NSA = ce_nsph(LA), NSB = ce_nsph(LB);
     static constexpr int NSC = ce_nsph(LC), NSD = ce_nsph(LD);
+    static constexpr int NSAB = NSA * NSB, NSCD = NSC * NSD;
+    static constexpr int TPQ = fast_pick_tpq(NAS, NCS);
+    static constexpr int BBQ = TPQ >= 4 ? 1 : 4 / TPQ;
+    static constexpr int WARPS = TPQ * BBQ;
+    // Phase-3 work split: by ket spherical function c when there are enough
+    // of them (K[ac], K[bc] complete inside one warp), else by column (c,d).
+    static constexpr bool BY_SC = NSC >= TPQ;
+    static constexpr int LANE_STRIDE = (NAS * NSCD) | 1;  // odd: conflict-free FP64 rows
+    static constexpr int SMEM_DOUBLES = TPQ == 1 ? 0 : BBQ * 32 * LANE_STRIDE;
 };
 
-// C(b,u) * x^(b-u) for small b, u (compile-time b, u).
-template <typename T>
-__device__ __forceinline__ T hrr_coef(int b, int u, T x) {
-    T c = T(1);
-    // binomial
+// Binomial C(n, k) for the small HRR exponents.
+__host__ __device__ constexpr int ce_binom(int n, int k) {
     int num = 1, den = 1;
-    for (int i = 0; i < u; ++i) { num *= (b - i); den *= (i + 1); }
-    c = T(num / den);
-    for (int i = 0; i < b - u; ++i) c *= x;
-    return c;
+    for (int i = 0; i < k; ++i) { num *= n - i; den *= i + 1; }
+    return num / den;
+}
+
+// Compile-time loop: f(integral_constant<int, 0>) ... f(integral_constant<int, N-1>),
+// so that every index derived from the loop variable is a constant expression
+// (register arrays stay in registers, no unroller/folding round trips).
+template <typename F, int... Is>
+__device__ __forceinline__ void sfor_seq(F&& f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void sfor(F&& f) {
+    if constexpr (N > 0) sfor_seq(f, std::make_integer_sequence<int, N>{});
+}
+#define TLNO_CI(x) decltype(x)::value
+
+// HRR transfer coefficient C(B,U) X^(B-U).
+template <int B, int U>
+__device__ __forceinline__ double hrr_coef(double x) {
+    constexpr int e = B - U;
+    constexpr double c = double(ce_binom(B, U));
+    if constexpr (e == 0) return 1.0;
+    else if constexpr (e == 1) return c * x;
+    else if constexpr (e == 2) return c * (x * x);
+    else if constexpr (e == 3) return c * (x * x * x);
+    else return c * ((x * x) * (x * x));
+}
+
+// Spherical element (S1, S2) of a shell pair (L1 >= L2) from the rows
+// (l1+u, 0) of its Cartesian range, l1 + u in [L1, L1+L2] (flat index minus
+// OF): horizontal transfer (a,b) = sum_u C(b,u) X^(b-u) (a+u, 0) with
+// X = centre1 - centre2, then the Cartesian->spherical projection with the
+// angular normalisation folded in.  src(integral_constant<int, f>) returns
+// row f.
+template <int L1, int L2, int S1, int S2, int OF, typename Src>
+__device__ __forceinline__ double pair_transfer(const double* X, Src&& src) {
+    double out = 0.0;
+    sfor<ce_ncart(L1)>([&](auto C1) {
+        constexpr int c1 = TLNO_CI(C1);
+        if constexpr (c2s_nz(L1, S1, c1)) {
+            constexpr int f1 = ce_off(L1) + c1;
+            double row = 0.0;
+            sfor<ce_ncart(L2)>([&](auto C2) {
+                constexpr int c2 = TLNO_CI(C2);
+                if constexpr (c2s_nz(L2, S2, c2)) {
+                    constexpr int f2 = ce_off(L2) + c2;
+                    constexpr int bx = ce_x(f2), by = ce_y(f2), bz = ce_z(f2);
+                    double h = 0.0;
+                    sfor<bx + 1>([&](auto UX) {
+                        sfor<by + 1>([&](auto UY) {
+                            sfor<bz + 1>([&](auto UZ) {
+                                constexpr int ux = TLNO_CI(UX), uy = TLNO_CI(UY), uz = TLNO_CI(UZ);
+                                constexpr int fu = ce_flat(ce_x(f1) + ux, ce_y(f1) + uy, ce_z(f1) + uz) - OF;
+                                h += hrr_coef<bx, ux>(X[0]) * hrr_coef<by, uy>(X[1]) * hrr_coef<bz, uz>(X[2]) *
+                                     src(std::integral_constant<int, fu>{});
+                            });
+                        });
+                    });
+                    if constexpr (L2 <= 1) row += h;
+                    else row += c_c2s.dense[L2][S2][c2] * h;
+                }
+            });
+            if constexpr (L1 <= 1) out += row;
+            else out += c_c2s.dense[L1][S1][c1] * row;
+        }
+    });
+    return out;
+}
+
+struct QuartetGeom {
+    double A[3], C[3];
+    double AB[3], CD[3];
+};
+
+// Phase 1 + 2 for slice G (rows ia = G, G+TPQ, ...).
+template <typename R, int LA, int LB, int LC, int LD, int G>
+__device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
+                                           double* __restrict__ ks) {
+    using S = FastShape<LA, LB, LC, LD>;
+    constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
+    R acc[ROWS > 0 ? ROWS : 1][S::NCS];
+#pragma unroll
+    for (int rr = 0; rr < ROWS; ++rr)
+#pragma unroll
+        for (int ic = 0; ic < S::NCS; ++ic) acc[rr][ic] = R(0);
+
+    if (active) {
+        const int npb = __ldg(pv.pair_nprim + bra), npk = __ldg(pv.pair_nprim + ket);
+        const DPrimPair* pb = pv.prim + __ldg(pv.pair_prim_off + bra);
+        const DPrimPair* pk = pv.prim + __ldg(pv.pair_prim_off + ket);
+        for (int ib = 0; ib < npb; ++ib) {
+            const double bp_p = __ldg(&pb[ib].p), bp_x = __ldg(&pb[ib].Px), bp_y = __ldg(&pb[ib].Py),
+                         bp_z = __ldg(&pb[ib].Pz), bp_w = __ldg(&pb[ib].w), bp_ip = __ldg(&pb[ib].invp);
+            const R p = R(bp_p);
+            const R PAx = R(bp_x - q.A[0]), PAy = R(bp_y - q.A[1]), PAz = R(bp_z - q.A[2]);
+            for (int ik = 0; ik < npk; ++ik) {
+                const double kp_p = __ldg(&pk[ik].p), kp_x = __ldg(&pk[ik].Px), kp_y = __ldg(&pk[ik].Py),
+                             kp_z = __ldg(&pk[ik].Pz), kp_w = __ldg(&pk[ik].w), kp_ip = __ldg(&pk[ik].invp);
+                const R qe = R(kp_p);
+                const R pqs = p + qe;
+                const R inv = R(1) / pqs;
+                const R PQx = R(bp_x - kp_x), PQy = R(bp_y - kp_y), PQz = R(bp_z - kp_z);
+                const R Targ = p * qe * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
+                R rt[S::N], wt[S::N];
+                rys_roots_all<R, S::N>(Targ, rt, wt);
+                const R pref = R(34.98683665524972497) * R(bp_w) * R(kp_w) * sqrt(inv);
+                const R qo = qe * inv, po = p * inv;
+                const R hbp = R(0.5) * R(bp_ip), hkp = R(0.5) * R(kp_ip);
+                const R QCx = R(kp_x - q.C[0]), QCy = R(kp_y - q.C[1]), QCz = R(kp_z - q.C[2]);
+#pragma unroll
+                for (int r = 0; r < S::N; ++r) {
+                    const R t2 = rt[r];
+                    const R b00 = R(0.5) * inv * t2;
+                    const R b10 = hbp - hbp * qo * t2;
+                    const R b01 = hkp - hkp * po * t2;
+                    const R qt = qo * t2, pt = po * t2;
+                    R g[3][S::GS];
+                    const R c00[3] = {PAx - qt * PQx, PAy - qt * PQy, PAz - qt * PQz};
+                    const R d00[3] = {QCx + pt * PQx, QCy + pt * PQy, QCz + pt * PQz};
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) {
+                        R* G2 = g[ax];
+                        G2[0] = (ax == 2) ? pref * wt[r] : R(1);
+                        if (S::LAB > 0) G2[S::KS] = c00[ax] * G2[0];
+#pragma unroll
+                        for (int ii = 1; ii < S::LAB; ++ii)
+                            G2[(ii + 1) * S::KS] = c00[ax] * G2[ii * S::KS] + R(ii) * b10 * G2[(ii - 1) * S::KS];
+#pragma unroll
+                        for (int k = 0; k < S::LCD; ++k) {
+#pragma unroll
+                            for (int ii = 0; ii <= S::LAB; ++ii) {
+                                R v = d00[ax] * G2[ii * S::KS + k];
+                                if (ii > 0) v += R(ii) * b00 * G2[(ii - 1) * S::KS + k];
+                                if (k > 0) v += R(k) * b01 * G2[ii * S::KS + k - 1];
+                                G2[ii * S::KS + k + 1] = v;
+                            }
+                        }
+                    }
+                    sfor<ROWS>([&](auto RR) {
+                        constexpr int rr = TLNO_CI(RR);
+                        constexpr int fa = S::OFA + G + rr * S::TPQ;
+                        constexpr int xa = ce_x(fa), ya = ce_y(fa), za = ce_z(fa);
+                        sfor<S::NCS>([&](auto IC) {
+                            constexpr int ic = TLNO_CI(IC);
+                            constexpr int fc = S::OFC + ic;
+                            acc[rr][ic] += (g[0][xa * S::KS + ce_x(fc)] * g[1][ya * S::KS + ce_y(fc)]) *
+                                           g[2][za * S::KS + ce_z(fc)];
+                        });
+                    });
+                }
+            }
+        }
+    }
+
+    // Phase 2: ket transfer + projection of the owned rows.
+    sfor<ROWS>([&](auto RR) {
+        constexpr int rr = TLNO_CI(RR);
+        constexpr int ia = G + rr * S::TPQ;
+        sfor<S::NSC>([&](auto SC) {
+            sfor<S::NSD>([&](auto SD) {
+                constexpr int sc = TLNO_CI(SC), sd = TLNO_CI(SD);
+                ks[ia * S::NSCD + sc * S::NSD + sd] = pair_transfer<LC, LD, sc, sd, S::OFC>(
+                    q.CD, [&](auto FU) { return double(acc[rr][TLNO_CI(FU)]); });
+            });
+        });
+    });
+}
+
+template <typename R, int LA, int LB, int LC, int LD, int G = 0>
+__device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, int bra, int ket, bool active,
+                                                    const QuartetGeom& q, double* ks) {
+    using S = FastShape<LA, LB, LC, LD>;
+    if constexpr (G < S::TPQ) {
+        if (g == G)
+            fast_slice<R, LA, LB, LC, LD, G>(pv, bra, ket, active, q, ks);
+        else
+            fast_slice_dispatch<R, LA, LB, LC, LD, G + 1>(g, pv, bra, ket, active, q, ks);
+    }
 }
 
 template <typename R, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) eri_fast_jk_kernel(PlanView pv, ClassLaunch cl) {
+__global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
+    eri_fast_jk_kernel(PlanView pv, ClassLaunch cl) {
     using S = FastShape<LA, LB, LC, LD>;
+    extern __shared__ double fast_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int grp = warp / S::TPQ, g = warp % S::TPQ;
+    // A quartet owned by one thread keeps its (a0|cd) rows in registers; a
+    // sliced quartet exchanges them through shared memory.
+    double ks_reg[S::TPQ == 1 ? S::NAS * S::NSCD : 1];
+    double* ks;
+    if constexpr (S::TPQ == 1)
+        ks = ks_reg;
+    else
+        ks = fast_smem + (grp * 32 + lane) * S::LANE_STRIDE;
     const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
+
     for (int tile = cl.tile_begin + blockIdx.x; tile < cl.tile_end; tile += gridDim.x) {
         const int b = find_block(cl.tile_prefix, cl.n_blocks, tile);
         const int kb = tile - __ldg(cl.tile_prefix + b);
         const BlockDesc bd = cl.blocks[b];
-        if (warp >= bd.nbra) continue;
-        const int i = bd.ilocal0 + warp;
+        const bool has_bra = grp < bd.nbra;
+        const int i = bd.ilocal0 + grp;
         const int j = kb * 32 + lane;
-        const int bra = bd.bra0 + warp;
-        const double qi = pv.pair_Q[bra];
-        bool active = j < bd.nket && !(cl.same && j > i);
+        const int bra = bd.bra0 + (has_bra ? grp : 0);
+        bool active = has_bra && j < bd.nket && !(cl.same && j > i);
         const int ket = bd.ket0 + (active ? j : 0);
         if (active) {
-            const double qq = qi * pv.pair_Q[ket];
+            const double qq = __ldg(pv.pair_Q + bra) * __ldg(pv.pair_Q + ket);
             active = qq >= cl.tau;
             if (cl.prec_mode == 1) active = active && qq >= thr;
             if (cl.prec_mode == 2) active = active && !(qq >= thr);
         }
-        if (!__any_sync(0xffffffffu, active)) continue;
+        bool any;
+        if constexpr (S::TPQ > 1)
+            any = __syncthreads_or(active) != 0;
+        else
+            any = __any_sync(0xffffffffu, active);
+        if (!any) continue;
 
-        const int A = pv.pair_A[bra], B = pv.pair_B[bra];
-        const int C = pv.pair_A[ket], D = pv.pair_B[ket];
-        const double Ax = pv.shell_xyz[3 * A], Ay = pv.shell_xyz[3 * A + 1], Az = pv.shell_xyz[3 * A + 2];
-        const double Cx = pv.shell_xyz[3 * C], Cy = pv.shell_xyz[3 * C + 1], Cz = pv.shell_xyz[3 * C + 2];
-
-        R Tr[S::NAS * S::NCS];
+        const int A = __ldg(pv.pair_A + bra), B = __ldg(pv.pair_B + bra);
+        const int C = __ldg(pv.pair_A + ket), D = __ldg(pv.pair_B + ket);
+        QuartetGeom q;
 #pragma unroll
-        for (int e = 0; e < S::NAS * S::NCS; ++e) Tr[e] = R(0);
-
-        if (active) {
-            const int npb = pv.pair_nprim[bra], npk = pv.pair_nprim[ket];
-            const DPrimPair* pb = pv.prim + pv.pair_prim_off[bra];
-            const DPrimPair* pk = pv.prim + pv.pair_prim_off[ket];
-            for (int ib = 0; ib < npb; ++ib) {
-                const DPrimPair bp = pb[ib];
-                const R p = R(bp.p);
-                const R PAx = R(bp.Px - Ax), PAy = R(bp.Py - Ay), PAz = R(bp.Pz - Az);
-                for (int ik = 0; ik < npk; ++ik) {
-                    const DPrimPair kp = pk[ik];
-                    const R q = R(kp.p);
-                    const R pqs = p + q;
-                    const R inv = R(1) / pqs;
-                    const R PQx = R(bp.Px - kp.Px), PQy = R(bp.Py - kp.Py), PQz = R(bp.Pz - kp.Pz);
-                    const R Targ = p * q * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
-                    R rt[S::N], wt[S::N];
-                    rys_roots_all<R, S::N>(Targ, rt, wt);
-                    const R pref = R(34.98683665524972497) * R(bp.w) * R(kp.w) / sqrt(pqs);
-                    const R qo = q * inv, po = p * inv;
-                    const R QCx = R(kp.Px - Cx), QCy = R(kp.Py - Cy), QCz = R(kp.Pz - Cz);
-#pragma unroll
-                    for (int r = 0; r < S::N; ++r) {
-                        const R t2 = rt[r];
-                        const R b00 = R(0.5) * inv * t2;
-                        const R b10 = R(0.5) * R(bp.invp) * (R(1) - qo * t2);
-                        const R b01 = R(0.5) * R(kp.invp) * (R(1) - po * t2);
-                        R G[3][S::GS];
-                        const R c00[3] = {PAx - qo * PQx * t2, PAy - qo * PQy * t2, PAz - qo * PQz * t2};
-                        const R d00[3] = {QCx + po * PQx * t2, QCy + po * PQy * t2, QCz + po * PQz * t2};
-#pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) {
-                            R* g = G[ax];
-                            g[0] = (ax == 2) ? pref * wt[r] : R(1);
-                            if (S::LAB > 0) g[S::KS] = c00[ax] * g[0];
-#pragma unroll
-                            for (int ii = 1; ii < S::LAB; ++ii)
-                                g[(ii + 1) * S::KS] = c00[ax] * g[ii * S::KS] + R(ii) * b10 * g[(ii - 1) * S::KS];
-#pragma unroll
-                            for (int k = 0; k < S::LCD; ++k) {
-#pragma unroll
-                                for (int ii = 0; ii <= S::LAB; ++ii) {
-                                    R v = d00[ax] * g[ii * S::KS + k];
-                                    if (ii > 0) v += R(ii) * b00 * g[(ii - 1) * S::KS + k];
-                                    if (k > 0) v += R(k) * b01 * g[ii * S::KS + k - 1];
-                                    g[ii * S::KS + k + 1] = v;
-                                }
-                            }
-                        }
-#pragma unroll
-                        for (int ia = 0; ia < S::NAS; ++ia) {
-#pragma unroll
-                            for (int ic = 0; ic < S::NCS; ++ic) {
-                                const int fa = S::OFA + ia, fc = S::OFC + ic;
-                                Tr[ia * S::NCS + ic] += G[0][ce_x(fa) * S::KS + ce_x(fc)] *
-                                                        G[1][ce_y(fa) * S::KS + ce_y(fc)] *
-                                                        G[2][ce_z(fa) * S::KS + ce_z(fc)];
-                            }
-                        }
-                    }
-                }
-            }
+        for (int k = 0; k < 3; ++k) {
+            q.A[k] = __ldg(pv.shell_xyz + 3 * A + k);
+            q.C[k] = __ldg(pv.shell_xyz + 3 * C + k);
+            q.AB[k] = q.A[k] - __ldg(pv.shell_xyz + 3 * B + k);
+            q.CD[k] = q.C[k] - __ldg(pv.shell_xyz + 3 * D + k);
         }
 
-        // Ket transfer K[ia][c][d] = sum_u C(d,u) CD^(d-u) T[ia][c+u], then the
-        // ket spherical projection, then the bra transfer and projection.
-        const double* xd = pv.shell_xyz + 3 * D;
-        const double* xb = pv.shell_xyz + 3 * B;
-        const double CD[3] = {Cx - xd[0], Cy - xd[1], Cz - xd[2]};
-        const double AB[3] = {Ax - xb[0], Ay - xb[1], Az - xb[2]};
-        constexpr int NSAB = S::NSA * S::NSB, NSCD = S::NSC * S::NSD;
-        double Ks[S::NAS * NSCD];
-#pragma unroll
-        for (int ia = 0; ia < S::NAS; ++ia) {
-            double Kc[S::NCC * S::NCD];
-#pragma unroll
-            for (int c = 0; c < S::NCC; ++c)
-#pragma unroll
-                for (int d = 0; d < S::NCD; ++d) {
-                    const int fc = ce_off(LC) + c, fd = ce_off(LD) + d;
-                    const int cxp = ce_x(fc), cyp = ce_y(fc), czp = ce_z(fc);
-                    const int dx = ce_x(fd), dy = ce_y(fd), dz = ce_z(fd);
-                    double s = 0.0;
-#pragma unroll
-                    for (int ux = 0; ux <= dx; ++ux)
-#pragma unroll
-                        for (int uy = 0; uy <= dy; ++uy)
-#pragma unroll
-                            for (int uz = 0; uz <= dz; ++uz) {
-                                const int fcu = ce_flat(cxp + ux, cyp + uy, czp + uz) - S::OFC;
-                                s += hrr_coef<double>(dx, ux, CD[0]) * hrr_coef<double>(dy, uy, CD[1]) *
-                                     hrr_coef<double>(dz, uz, CD[2]) * double(Tr[ia * S::NCS + fcu]);
-                            }
-                    Kc[c * S::NCD + d] = s;
-                }
-#pragma unroll
-            for (int sc = 0; sc < S::NSC; ++sc)
-#pragma unroll
-                for (int sd = 0; sd < S::NSD; ++sd) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int c = 0; c < S::NCC; ++c)
-#pragma unroll
-                        for (int d = 0; d < S::NCD; ++d) {
-                            if ((LC <= 1 && c != sc) || (LD <= 1 && d != sd)) continue;
-                            const double kc = (LC <= 1) ? 1.0 : c_c2s.dense[LC][sc][c];
-                            const double kd = (LD <= 1) ? 1.0 : c_c2s.dense[LD][sd][d];
-                            s += kc * kd * Kc[c * S::NCD + d];
-                        }
-                    Ks[ia * NSCD + sc * S::NSD + sd] = s;
-                }
-        }
-        double V[NSAB * NSCD];
-#pragma unroll
-        for (int t = 0; t < NSCD; ++t) {
-            double Vc[S::NCA * S::NCB];
-#pragma unroll
-            for (int a = 0; a < S::NCA; ++a)
-#pragma unroll
-                for (int bq = 0; bq < S::NCB; ++bq) {
-                    const int fa = ce_off(LA) + a, fb = ce_off(LB) + bq;
-                    const int axp = ce_x(fa), ayp = ce_y(fa), azp = ce_z(fa);
-                    const int bx = ce_x(fb), by = ce_y(fb), bz = ce_z(fb);
-                    double s = 0.0;
-#pragma unroll
-                    for (int ux = 0; ux <= bx; ++ux)
-#pragma unroll
-                        for (int uy = 0; uy <= by; ++uy)
-#pragma unroll
-                            for (int uz = 0; uz <= bz; ++uz) {
-                                const int fau = ce_flat(axp + ux, ayp + uy, azp + uz) - S::OFA;
-                                s += hrr_coef<double>(bx, ux, AB[0]) * hrr_coef<double>(by, uy, AB[1]) *
-                                     hrr_coef<double>(bz, uz, AB[2]) * Ks[fau * NSCD + t];
-                            }
-                    Vc[a * S::NCB + bq] = s;
-                }
-#pragma unroll
-            for (int sa = 0; sa < S::NSA; ++sa)
-#pragma unroll
-                for (int sb = 0; sb < S::NSB; ++sb) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int a = 0; a < S::NCA; ++a)
-#pragma unroll
-                        for (int bq = 0; bq < S::NCB; ++bq) {
-                            if ((LA <= 1 && a != sa) || (LB <= 1 && bq != sb)) continue;
-                            const double ka = (LA <= 1) ? 1.0 : c_c2s.dense[LA][sa][a];
-                            const double kb = (LB <= 1) ? 1.0 : c_c2s.dense[LB][sb][bq];
-                            s += ka * kb * Vc[a * S::NCB + bq];
-                        }
-                    V[(sa * S::NSB + sb) * NSCD + t] = s;
-                }
-        }
+        fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, ks);
+        if constexpr (S::TPQ > 1) __syncthreads();
 
-        // ---- digestion ----
-        const int mol = pv.pair_mol ? pv.pair_mol[bra] : 0;
-        const int M = pv.mol_M ? pv.mol_M[mol] : cl.M;
-        const long long mbase = pv.mol_mat_off ? pv.mol_mat_off[mol] : 0;
+        // ---- phase 3: bra transfer + projection per owned ket column, digestion ----
+        const int mol = pv.pair_mol ? __ldg(pv.pair_mol + bra) : 0;
+        const int M = pv.mol_M ? __ldg(pv.mol_M + mol) : cl.M;
+        const long long mbase = pv.mol_mat_off ? __ldg(pv.mol_mat_off + mol) : 0;
         const double* Dm = cl.dens + mbase;
         double* Jm = cl.J + mbase;
         double* Km = cl.K + mbase;
-        const int a0 = pv.shell_sph[A], b0 = pv.shell_sph[B];
-        const int c0 = pv.shell_sph[C], d0 = pv.shell_sph[D];
+        const int a0 = __ldg(pv.shell_sph + A), b0 = __ldg(pv.shell_sph + B);
+        const int c0 = __ldg(pv.shell_sph + C), d0 = __ldg(pv.shell_sph + D);
         double f = active ? 1.0 : 0.0;
         if (A == B) f *= 0.5;
         if (C == D) f *= 0.5;
         if (bra == ket) f *= 0.5;
-        if (cl.want_j) {
-            double Pab[NSAB];
+        const double fj = 4.0 * f, fk = 2.0 * f;
+        auto dm = [&](int r, int c) { return __ldg(Dm + (long long)r * M + c); };
+
+        double jab[S::NSAB];
 #pragma unroll
-            for (int e = 0; e < NSAB; ++e) Pab[e] = __ldg(Dm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB);
+        for (int e = 0; e < S::NSAB; ++e) jab[e] = 0.0;
+
+        if (active) {
+            double kad[S::NSA][S::NSD], kbd[S::NSB][S::NSD];
 #pragma unroll
-            for (int sab = 0; sab < NSAB; ++sab) {
-                double s = 0.0;
-                if (active) {
+            for (int sd = 0; sd < S::NSD; ++sd) {
 #pragma unroll
-                    for (int t = 0; t < NSCD; ++t)
-                        s += V[sab * NSCD + t] * __ldg(Dm + (long long)(c0 + t / S::NSD) * M + d0 + t % S::NSD);
+                for (int a = 0; a < S::NSA; ++a) kad[a][sd] = 0.0;
+#pragma unroll
+                for (int bq = 0; bq < S::NSB; ++bq) kbd[bq][sd] = 0.0;
+            }
+            sfor<S::NSC>([&](auto SC) {
+                constexpr int sc = TLNO_CI(SC);
+                double kac[S::NSA], kbc[S::NSB];
+#pragma unroll
+                for (int a = 0; a < S::NSA; ++a) kac[a] = 0.0;
+#pragma unroll
+                for (int bq = 0; bq < S::NSB; ++bq) kbc[bq] = 0.0;
+                bool own_sc = false;
+                sfor<S::NSD>([&](auto SD) {
+                    constexpr int sd = TLNO_CI(SD);
+                    constexpr int t = sc * S::NSD + sd;
+                    const bool own = S::BY_SC ? (sc % S::TPQ == g) : (t % S::TPQ == g);
+                    if (!own) return;
+                    own_sc = true;
+                    double V[S::NSAB];
+                    sfor<S::NSA>([&](auto SA) {
+                        sfor<S::NSB>([&](auto SB) {
+                            constexpr int sa = TLNO_CI(SA), sb = TLNO_CI(SB);
+                            V[sa * S::NSB + sb] = pair_transfer<LA, LB, sa, sb, S::OFA>(
+                                q.AB, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
+                        });
+                    });
+                    if (cl.want_j) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int e = 0; e < S::NSAB; ++e) s += V[e] * dm(a0 + e / S::NSB, b0 + e % S::NSB);
+                        atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, fj * s);
+                        const double dcd = dm(c0 + sc, d0 + sd);
+#pragma unroll
+                        for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
+                    }
+                    if (cl.want_k) {
+#pragma unroll
+                        for (int sa = 0; sa < S::NSA; ++sa) {
+                            const double dad = dm(a0 + sa, d0 + sd), dac = dm(a0 + sa, c0 + sc);
+#pragma unroll
+                            for (int sb = 0; sb < S::NSB; ++sb) {
+                                const double v = V[sa * S::NSB + sb];
+                                kac[sa] += v * dm(b0 + sb, d0 + sd);
+                                kad[sa][sd] += v * dm(b0 + sb, c0 + sc);
+                                kbc[sb] += v * dad;
+                                kbd[sb][sd] += v * dac;
+                            }
+                        }
+                    }
+                });
+                if (cl.want_k && own_sc) {
+#pragma unroll
+                    for (int sa = 0; sa < S::NSA; ++sa) atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, fk * kac[sa]);
+#pragma unroll
+                    for (int sb = 0; sb < S::NSB; ++sb) atomicAdd(Km + (long long)(b0 + sb) * M + c0 + sc, fk * kbc[sb]);
                 }
-                s *= 4.0 * f;
+            });
+            if (cl.want_k) {
+                sfor<S::NSD>([&](auto SD) {
+                    constexpr int sd = TLNO_CI(SD);
+                    bool own_d = false;
+#pragma unroll
+                    for (int sc = 0; sc < S::NSC; ++sc)
+                        own_d = own_d || (S::BY_SC ? (sc % S::TPQ == g) : ((sc * S::NSD + sd) % S::TPQ == g));
+                    if (!own_d) return;
+#pragma unroll
+                    for (int sa = 0; sa < S::NSA; ++sa) atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, fk * kad[sa][sd]);
+#pragma unroll
+                    for (int sb = 0; sb < S::NSB; ++sb) atomicAdd(Km + (long long)(b0 + sb) * M + d0 + sd, fk * kbd[sb][sd]);
+                });
+            }
+        }
+        if (cl.want_j) {
+            // J[ab]: every lane of the warp shares the bra pair.
+#pragma unroll
+            for (int e = 0; e < S::NSAB; ++e) {
+                double s = fj * jab[e];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) atomicAdd(Jm + (long long)(a0 + sab / S::NSB) * M + b0 + sab % S::NSB, s);
-            }
-            if (active) {
-#pragma unroll
-                for (int t = 0; t < NSCD; ++t) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int sab = 0; sab < NSAB; ++sab) s += V[sab * NSCD + t] * Pab[sab];
-                    atomicAdd(Jm + (long long)(c0 + t / S::NSD) * M + d0 + t % S::NSD, 4.0 * f * s);
-                }
+                if (lane == 0 && has_bra && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
             }
         }
-        if (cl.want_k && active) {
-            const double fk = 2.0 * f;
-#pragma unroll
-            for (int a = 0; a < S::NSA; ++a)
-#pragma unroll
-                for (int c = 0; c < S::NSC; ++c) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int bq = 0; bq < S::NSB; ++bq)
-#pragma unroll
-                        for (int d = 0; d < S::NSD; ++d)
-                            s += V[(a * S::NSB + bq) * NSCD + c * S::NSD + d] * __ldg(Dm + (long long)(b0 + bq) * M + d0 + d);
-                    atomicAdd(Km + (long long)(a0 + a) * M + c0 + c, fk * s);
-                }
-#pragma unroll
-            for (int a = 0; a < S::NSA; ++a)
-#pragma unroll
-                for (int d = 0; d < S::NSD; ++d) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int bq = 0; bq < S::NSB; ++bq)
-#pragma unroll
-                        for (int c = 0; c < S::NSC; ++c)
-                            s += V[(a * S::NSB + bq) * NSCD + c * S::NSD + d] * __ldg(Dm + (long long)(b0 + bq) * M + c0 + c);
-                    atomicAdd(Km + (long long)(a0 + a) * M + d0 + d, fk * s);
-                }
-#pragma unroll
-            for (int bq = 0; bq < S::NSB; ++bq)
-#pragma unroll
-                for (int c = 0; c < S::NSC; ++c) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int a = 0; a < S::NSA; ++a)
-#pragma unroll
-                        for (int d = 0; d < S::NSD; ++d)
-                            s += V[(a * S::NSB + bq) * NSCD + c * S::NSD + d] * __ldg(Dm + (long long)(a0 + a) * M + d0 + d);
-                    atomicAdd(Km + (long long)(b0 + bq) * M + c0 + c, fk * s);
-                }
-#pragma unroll
-            for (int bq = 0; bq < S::NSB; ++bq)
-#pragma unroll
-                for (int d = 0; d < S::NSD; ++d) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int a = 0; a < S::NSA; ++a)
-#pragma unroll
-                        for (int c = 0; c < S::NSC; ++c)
-                            s += V[(a * S::NSB + bq) * NSCD + c * S::NSD + d] * __ldg(Dm + (long long)(a0 + a) * M + c0 + c);
-                    atomicAdd(Km + (long long)(b0 + bq) * M + d0 + d, fk * s);
-                }
-        }
+        if constexpr (S::TPQ > 1) __syncthreads();
     }
 }
+
+// Launch geometry of class (la lb|lc ld) for the host.
+template <int LA, int LB, int LC, int LD>
+constexpr int fast_warps() { return FastShape<LA, LB, LC, LD>::WARPS; }
+template <int LA, int LB, int LC, int LD>
+constexpr int fast_bras() { return FastShape<LA, LB, LC, LD>::BBQ; }
+template <int LA, int LB, int LC, int LD>
+constexpr int fast_smem_bytes() { return FastShape<LA, LB, LC, LD>::SMEM_DOUBLES * 8; }
 
 }  // namespace dev
 }  // namespace tlno_gpu

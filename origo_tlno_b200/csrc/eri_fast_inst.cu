@@ -14,16 +14,26 @@
 
 namespace tlno_gpu {
 
-#define TLNO_FAST_IMPL(id, a, b, c, d)                                                                 \
-    void fast_upload_##id(const dev::DevTables& t, const dev::CartTable& ct, const dev::C2STable& cs) { \
-        dev::upload_constant_tables(t, ct, cs);                                                        \
-    }                                                                                                  \
-    void fast_launch_##id(bool fp32, const dev::PlanView& pv, const dev::ClassLaunch& cl, int grid,    \
-                          int threads, cudaStream_t s) {                                               \
-        if (fp32)                                                                                      \
-            dev::eri_fast_jk_kernel<float, a, b, c, d><<<grid, threads, 0, s>>>(pv, cl);               \
-        else                                                                                           \
-            dev::eri_fast_jk_kernel<double, a, b, c, d><<<grid, threads, 0, s>>>(pv, cl);              \
+#define TLNO_FAST_IMPL(id, a, b, c, d)                                                                  \
+    void fast_upload_##id(const dev::DevTables& t, const dev::CartTable& ct, const dev::C2STable& cs) {  \
+        dev::upload_constant_tables(t, ct, cs);                                                         \
+        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
+        if (smem > 48 * 1024) {                                                                         \
+            cudaFuncSetAttribute(dev::eri_fast_jk_kernel<double, a, b, c, d>,                           \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);                    \
+            cudaFuncSetAttribute(dev::eri_fast_jk_kernel<float, a, b, c, d>,                            \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);                    \
+        }                                                                                               \
+    }                                                                                                   \
+    int fast_bras_##id() { return dev::fast_bras<a, b, c, d>(); }                                       \
+    void fast_launch_##id(bool fp32, const dev::PlanView& pv, const dev::ClassLaunch& cl, int grid,     \
+                          cudaStream_t s) {                                                             \
+        constexpr int threads = 32 * dev::fast_warps<a, b, c, d>();                                     \
+        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
+        if (fp32)                                                                                       \
+            dev::eri_fast_jk_kernel<float, a, b, c, d><<<grid, threads, smem, s>>>(pv, cl);             \
+        else                                                                                            \
+            dev::eri_fast_jk_kernel<double, a, b, c, d><<<grid, threads, smem, s>>>(pv, cl);            \
     }
 
 #define TLNO_FAST_SELECT(id, a, b, c, d) \
@@ -83,6 +93,46 @@ namespace tlno_gpu {
 #define TLNO_FAST_IF_10(x) x
 #else
 #define TLNO_FAST_IF_10(x)
+#endif
+#if TLNO_FAST_ID == 11
+#define TLNO_FAST_IF_11(x) x
+#else
+#define TLNO_FAST_IF_11(x)
+#endif
+#if TLNO_FAST_ID == 12
+#define TLNO_FAST_IF_12(x) x
+#else
+#define TLNO_FAST_IF_12(x)
+#endif
+#if TLNO_FAST_ID == 13
+#define TLNO_FAST_IF_13(x) x
+#else
+#define TLNO_FAST_IF_13(x)
+#endif
+#if TLNO_FAST_ID == 14
+#define TLNO_FAST_IF_14(x) x
+#else
+#define TLNO_FAST_IF_14(x)
+#endif
+#if TLNO_FAST_ID == 15
+#define TLNO_FAST_IF_15(x) x
+#else
+#define TLNO_FAST_IF_15(x)
+#endif
+#if TLNO_FAST_ID == 16
+#define TLNO_FAST_IF_16(x) x
+#else
+#define TLNO_FAST_IF_16(x)
+#endif
+#if TLNO_FAST_ID == 17
+#define TLNO_FAST_IF_17(x) x
+#else
+#define TLNO_FAST_IF_17(x)
+#endif
+#if TLNO_FAST_ID == 18
+#define TLNO_FAST_IF_18(x) x
+#else
+#define TLNO_FAST_IF_18(x)
 #endif
 
 TLNO_FAST_CLASSES(TLNO_FAST_SELECT)

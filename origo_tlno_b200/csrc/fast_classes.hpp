@@ -1,7 +1,8 @@
-// Classes with a thread-per-quartet ERI kernel (la >= lb, lc >= ld, bra
-// class index >= ket class index), chosen so that their contracted radial
-// accumulators fit in registers.  Each class is compiled in its own
-// translation unit (eri_fast_inst.cu with -DTLNO_FAST_ID=<index>).
+// Classes with a compile-time ERI kernel (la >= lb, lc >= ld, bra class
+// index >= ket class index): every class with all shells up to d except
+// (dd|dp) and (dd|dd), which take the warp-per-quartet kernel.  Each class is
+// compiled in its own translation unit (eri_fast_inst.cu with
+// -DTLNO_FAST_ID=<index>).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -12,14 +13,22 @@
     X(2, 1, 0, 1, 0)         \
     X(3, 1, 1, 0, 0)         \
     X(4, 1, 1, 1, 0)         \
-    X(5, 2, 0, 0, 0)         \
-    X(6, 2, 0, 1, 0)         \
-    X(7, 2, 0, 1, 1)         \
-    X(8, 2, 0, 2, 0)         \
-    X(9, 2, 1, 0, 0)         \
-    X(10, 2, 2, 0, 0)
+    X(5, 1, 1, 1, 1)         \
+    X(6, 2, 0, 0, 0)         \
+    X(7, 2, 0, 1, 0)         \
+    X(8, 2, 0, 1, 1)         \
+    X(9, 2, 0, 2, 0)         \
+    X(10, 2, 1, 0, 0)        \
+    X(11, 2, 1, 1, 0)        \
+    X(12, 2, 1, 1, 1)        \
+    X(13, 2, 1, 2, 0)        \
+    X(14, 2, 1, 2, 1)        \
+    X(15, 2, 2, 0, 0)        \
+    X(16, 2, 2, 1, 0)        \
+    X(17, 2, 2, 1, 1)        \
+    X(18, 2, 2, 2, 0)
 
-#define TLNO_FAST_COUNT 11
+#define TLNO_FAST_COUNT 19
 
 namespace tlno_gpu {
 namespace dev {
@@ -33,8 +42,8 @@ struct ClassLaunch;
 // Defined once per class by eri_fast_inst.cu.
 #define TLNO_FAST_DECL(id, a, b, c, d)                                                          \
     void fast_upload_##id(const dev::DevTables&, const dev::CartTable&, const dev::C2STable&); \
-    void fast_launch_##id(bool fp32, const dev::PlanView&, const dev::ClassLaunch&, int grid,   \
-                          int threads, cudaStream_t s);
+    int fast_bras_##id();                                                                      \
+    void fast_launch_##id(bool fp32, const dev::PlanView&, const dev::ClassLaunch&, int grid, cudaStream_t s);
 TLNO_FAST_CLASSES(TLNO_FAST_DECL)
 #undef TLNO_FAST_DECL
 

@@ -329,6 +329,16 @@ void launch_eri_jk_generic(const PlanView& pv, const ClassLaunch& cl, bool fp32,
 
 bool has_fast_kernel(int la, int lb, int lc, int ld) { return fast_class_index(la, lb, lc, ld) >= 0; }
 
+int fast_kernel_bras(int la, int lb, int lc, int ld) {
+    switch (fast_class_index(la, lb, lc, ld)) {
+#define TLNO_FAST_BRAS(id, a, b, c, d) \
+    case id: return fast_bras_##id();
+        TLNO_FAST_CLASSES(TLNO_FAST_BRAS)
+#undef TLNO_FAST_BRAS
+        default: return 1;
+    }
+}
+
 bool launch_eri_jk_fast(const PlanView& pv, const ClassLaunch& cl, bool fp32, int grid, cudaStream_t s) {
     const int idx = fast_class_index(cl.la, cl.lb, cl.lc, cl.ld);
     if (idx < 0) return false;
@@ -336,10 +346,9 @@ bool launch_eri_jk_fast(const PlanView& pv, const ClassLaunch& cl, bool fp32, in
     const int ntiles = cl.tile_end - cl.tile_begin;
     if (grid <= 0) grid = sm_count() * 8;
     grid = std::min(grid, ntiles);
-    const int threads = 32 * cl.bb;
     switch (idx) {
 #define TLNO_FAST_CASE(id, a, b, c, d) \
-    case id: fast_launch_##id(fp32, pv, cl, grid, threads, s); break;
+    case id: fast_launch_##id(fp32, pv, cl, grid, s); break;
         TLNO_FAST_CLASSES(TLNO_FAST_CASE)
 #undef TLNO_FAST_CASE
         default: return false;

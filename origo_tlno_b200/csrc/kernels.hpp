@@ -27,6 +27,9 @@ void launch_eri_jk_generic(const dev::PlanView& pv, const dev::ClassLaunch& cl, 
 bool launch_eri_jk_fast(const dev::PlanView& pv, const dev::ClassLaunch& cl, bool fp32,
                         int grid, cudaStream_t s);
 bool has_fast_kernel(int la, int lb, int lc, int ld);
+// Bra pairs per CTA of the compile-time kernel of a class (its schedule's
+// block height).
+int fast_kernel_bras(int la, int lb, int lc, int ld);
 
 void launch_onee(const dev::OneeLaunch& L, cudaStream_t s);
 // out = (X + X^T) / 2 for `count` stacked M x M blocks (offsets per block).

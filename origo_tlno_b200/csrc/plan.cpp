@@ -358,7 +358,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
             const int combo_id = X * kMaxPairClasses + Y;
             cs.fast = has_fast_kernel(cs.la, cs.lb, cs.lc, cs.ld) &&
                       !(combo_id < 256 && tune.force_generic[combo_id]);
-            cs.bb = cs.fast ? tune.fast_bb : 1;
+            cs.bb = cs.fast ? fast_kernel_bras(cs.la, cs.lb, cs.lc, cs.ld) : 1;
             cs.bk = cs.fast ? 32 : tune.generic_bk;
             const double fprim = flops_per_prim(cs.la, cs.lb, cs.lc, cs.ld);
             const double fcon = flops_per_contracted(cs.la, cs.lb, cs.lc, cs.ld);
