@@ -17,10 +17,12 @@ constexpr int kMaxRoots = 9;
 
 struct DevTables {
     const double* boys;             // [row * 40 + n]
-    const double* rys_r[kMaxRoots + 1];
-    const double* rys_w[kMaxRoots + 1];
-    const float* rys_r32[kMaxRoots + 1];
-    const float* rys_w32[kMaxRoots + 1];
+    // Rys roots/weights per root count N as local quartic polynomials: grid
+    // point k holds 5 coefficient rows of 2N values (N roots, then N
+    // weights), record [(k * 5 + j) * 2N + i], so one lookup reads one
+    // contiguous 80N-byte record (40N bytes in FP32).
+    const double* rys_h[kMaxRoots + 1];
+    const float* rys_h32[kMaxRoots + 1];
     double tmax[kMaxRoots + 1];
     double h2[kMaxRoots + 1][kMaxRoots];
     double hw[kMaxRoots + 1][kMaxRoots];
@@ -111,27 +113,21 @@ __device__ __forceinline__ void boys_fn(int maxn, double x, double* F) {
 }
 
 // ---------------------------------------------------------------------------
-// Rys root t_i^2 and weight w_i (i < N) for argument T.  Below tmax(N) a
-// 5-point Newton-forward stencil on the 0.01 grid (the reference's scheme,
-// rys_engine.ipp:3784-3812); above it the Hermite asymptotic form.
+// Rys root t_i^2 and weight w_i (i < N) for argument T.  Below tmax(N) the
+// 5-point Newton-forward interpolant on the 0.01 grid (the reference's
+// scheme, rys_engine.ipp:3784-3812), stored in power form
+// c0 + c1 t + ... + c4 t^4 of the offset t in [0, 1) so that one lookup is
+// one contiguous record and four FMAs per value; above tmax the Hermite
+// asymptotic form.
 template <typename R> struct RysTab;
 template <> struct RysTab<double> {
-    static __device__ __forceinline__ const double* r(int n) { return c_tabs.rys_r[n]; }
-    static __device__ __forceinline__ const double* w(int n) { return c_tabs.rys_w[n]; }
+    using V2 = double2;
+    static __device__ __forceinline__ const double* h(int n) { return c_tabs.rys_h[n]; }
 };
 template <> struct RysTab<float> {
-    static __device__ __forceinline__ const float* r(int n) { return c_tabs.rys_r32[n]; }
-    static __device__ __forceinline__ const float* w(int n) { return c_tabs.rys_w32[n]; }
+    using V2 = float2;
+    static __device__ __forceinline__ const float* h(int n) { return c_tabs.rys_h32[n]; }
 };
-
-template <typename R>
-__device__ __forceinline__ R newton5(R f0, R f1, R f2, R f3, R f4, R t) {
-    const R d1 = f1 - f0;
-    const R d2 = (f2 - R(2) * f1 + f0) * R(0.5);
-    const R d3 = (f3 - R(3) * f2 + R(3) * f1 - f0) * R(1.0 / 6.0);
-    const R d4 = (f4 - R(4) * f3 + R(6) * f2 - R(4) * f1 + f0) * R(1.0 / 24.0);
-    return f0 + t * (d1 + (t - R(1)) * (d2 + (t - R(2)) * (d3 + (t - R(3)) * d4)));
-}
 
 template <typename R>
 __device__ __forceinline__ void rys_root(int N, R T, int i, R& root, R& weight) {
@@ -144,13 +140,18 @@ __device__ __forceinline__ void rys_root(int N, R T, int i, R& root, R& weight) 
     const R fi = T * R(100);
     const int k = static_cast<int>(fi);
     const R t = fi - R(k);
-    const R* rb = RysTab<R>::r(N) + k * N + i;
-    const R* wb = RysTab<R>::w(N) + k * N + i;
-    root = newton5<R>(__ldg(rb), __ldg(rb + N), __ldg(rb + 2 * N), __ldg(rb + 3 * N), __ldg(rb + 4 * N), t);
-    weight = newton5<R>(__ldg(wb), __ldg(wb + N), __ldg(wb + 2 * N), __ldg(wb + 3 * N), __ldg(wb + 4 * N), t);
+    const R* rec = RysTab<R>::h(N) + static_cast<long long>(k) * 10 * N;
+    R r = __ldg(rec + 8 * N + i), w = __ldg(rec + 9 * N + i);
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+        r = r * t + __ldg(rec + 2 * j * N + i);
+        w = w * t + __ldg(rec + (2 * j + 1) * N + i);
+    }
+    root = r;
+    weight = w;
 }
 
-// All N roots at once (thread-per-quartet kernels).
+// All N roots at once (compile-time N).
 template <typename R, int N>
 __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
     if (T >= R(c_tabs.tmax[N])) {
@@ -163,17 +164,28 @@ __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
         }
         return;
     }
+    using V2 = typename RysTab<R>::V2;
     const R fi = T * R(100);
     const int k = static_cast<int>(fi);
     const R t = fi - R(k);
-    const R* rb = RysTab<R>::r(N) + k * N;
-    const R* wb = RysTab<R>::w(N) + k * N;
+    const V2* rec = reinterpret_cast<const V2*>(RysTab<R>::h(N) + static_cast<long long>(k) * 10 * N);
+    R c[5][2 * N];
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-        root[i] = newton5<R>(__ldg(rb + i), __ldg(rb + N + i), __ldg(rb + 2 * N + i),
-                             __ldg(rb + 3 * N + i), __ldg(rb + 4 * N + i), t);
-        weight[i] = newton5<R>(__ldg(wb + i), __ldg(wb + N + i), __ldg(wb + 2 * N + i),
-                               __ldg(wb + 3 * N + i), __ldg(wb + 4 * N + i), t);
+    for (int j = 0; j < 5; ++j)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const V2 v = __ldg(rec + j * N + m);
+            c[j][2 * m] = v.x;
+            c[j][2 * m + 1] = v.y;
+        }
+#pragma unroll
+    for (int i = 0; i < 2 * N; ++i) {
+        R v = c[4][i];
+        v = v * t + c[3][i];
+        v = v * t + c[2][i];
+        v = v * t + c[1][i];
+        v = v * t + c[0][i];
+        if (i < N) root[i] = v; else weight[i - N] = v;
     }
 }
 

@@ -199,24 +199,27 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
     if (active) {
         const int npb = __ldg(pv.pair_nprim + bra), npk = __ldg(pv.pair_nprim + ket);
-        const DPrimPair* pb = pv.prim + __ldg(pv.pair_prim_off + bra);
-        const DPrimPair* pk = pv.prim + __ldg(pv.pair_prim_off + ket);
+        // 48-byte records {p, Px, Py, Pz, w, 1/p} read as three 16-byte vectors.
+        const double2* pb = reinterpret_cast<const double2*>(pv.prim + __ldg(pv.pair_prim_off + bra));
+        const double2* pk = reinterpret_cast<const double2*>(pv.prim + __ldg(pv.pair_prim_off + ket));
         for (int ib = 0; ib < npb; ++ib) {
-            const double bp_p = __ldg(&pb[ib].p), bp_x = __ldg(&pb[ib].Px), bp_y = __ldg(&pb[ib].Py),
-                         bp_z = __ldg(&pb[ib].Pz), bp_w = __ldg(&pb[ib].w), bp_ip = __ldg(&pb[ib].invp);
+            const double2 b0v = __ldg(pb + 3 * ib), b1v = __ldg(pb + 3 * ib + 1), b2v = __ldg(pb + 3 * ib + 2);
+            const double bp_p = b0v.x, bp_x = b0v.y, bp_y = b1v.x, bp_z = b1v.y, bp_w = b2v.x, bp_ip = b2v.y;
             const R p = R(bp_p);
             const R PAx = R(bp_x - q.A[0]), PAy = R(bp_y - q.A[1]), PAz = R(bp_z - q.A[2]);
             for (int ik = 0; ik < npk; ++ik) {
-                const double kp_p = __ldg(&pk[ik].p), kp_x = __ldg(&pk[ik].Px), kp_y = __ldg(&pk[ik].Py),
-                             kp_z = __ldg(&pk[ik].Pz), kp_w = __ldg(&pk[ik].w), kp_ip = __ldg(&pk[ik].invp);
+                const double2 k0v = __ldg(pk + 3 * ik), k1v = __ldg(pk + 3 * ik + 1), k2v = __ldg(pk + 3 * ik + 2);
+                const double kp_p = k0v.x, kp_x = k0v.y, kp_y = k1v.x, kp_z = k1v.y, kp_w = k2v.x, kp_ip = k2v.y;
                 const R qe = R(kp_p);
                 const R pqs = p + qe;
-                const R inv = R(1) / pqs;
+                // one reciprocal square root gives both 1/sqrt(p+q) and 1/(p+q)
+                const R rs = rsqrt(pqs);
+                const R inv = rs * rs;
                 const R PQx = R(bp_x - kp_x), PQy = R(bp_y - kp_y), PQz = R(bp_z - kp_z);
                 const R Targ = p * qe * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
                 R rt[S::N], wt[S::N];
                 rys_roots_all<R, S::N>(Targ, rt, wt);
-                const R pref = R(34.98683665524972497) * R(bp_w) * R(kp_w) * sqrt(inv);
+                const R pref = R(34.98683665524972497) * R(bp_w) * R(kp_w) * rs;
                 const R qo = qe * inv, po = p * inv;
                 const R hbp = R(0.5) * R(bp_ip), hkp = R(0.5) * R(kp_ip);
                 const R QCx = R(kp_x - q.C[0]), QCy = R(kp_y - q.C[1]), QCz = R(kp_z - q.C[2]);

@@ -26,6 +26,18 @@ namespace tlno_gpu {
         }                                                                                               \
     }                                                                                                   \
     int fast_bras_##id() { return dev::fast_bras<a, b, c, d>(); }                                       \
+    int fast_blocks_per_sm_##id(bool fp32) {                                                            \
+        constexpr int threads = 32 * dev::fast_warps<a, b, c, d>();                                     \
+        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
+        int n = 0;                                                                                      \
+        if (fp32)                                                                                       \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::eri_fast_jk_kernel<float, a, b, c, d>, \
+                                                          threads, smem);                               \
+        else                                                                                            \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::eri_fast_jk_kernel<double, a, b, c, d>, \
+                                                          threads, smem);                               \
+        return n > 0 ? n : 1;                                                                           \
+    }                                                                                                   \
     void fast_launch_##id(bool fp32, const dev::PlanView& pv, const dev::ClassLaunch& cl, int grid,     \
                           cudaStream_t s) {                                                             \
         constexpr int threads = 32 * dev::fast_warps<a, b, c, d>();                                     \

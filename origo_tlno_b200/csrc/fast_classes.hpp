@@ -43,6 +43,7 @@ struct ClassLaunch;
 #define TLNO_FAST_DECL(id, a, b, c, d)                                                          \
     void fast_upload_##id(const dev::DevTables&, const dev::CartTable&, const dev::C2STable&); \
     int fast_bras_##id();                                                                      \
+    int fast_blocks_per_sm_##id(bool fp32);                                                    \
     void fast_launch_##id(bool fp32, const dev::PlanView&, const dev::ClassLaunch&, int grid, cudaStream_t s);
 TLNO_FAST_CLASSES(TLNO_FAST_DECL)
 #undef TLNO_FAST_DECL

@@ -226,6 +226,34 @@ __global__ void fma_peak_kernel(R* out, int iters, R seed) {
     if (s == R(-12345)) out[0] = s;  // keeps the chains live
 }
 
+// Power-form records of the 5-point Newton-forward interpolant on rows
+// k..k+4 of the Rys table: with forward differences d1 = D f0,
+// d2 = D^2 f0 / 2, d3 = D^3 f0 / 6, d4 = D^4 f0 / 24,
+//   p(t) = f0 + d1 t + d2 t(t-1) + d3 t(t-1)(t-2) + d4 t(t-1)(t-2)(t-3)
+//        = c0 + c1 t + c2 t^2 + c3 t^3 + c4 t^4,
+//   c1 = d1 - d2 + 2 d3 - 6 d4, c2 = d2 - 3 d3 + 11 d4, c3 = d3 - 6 d4, c4 = d4.
+// Record k: [(k * 5 + j) * 2N + i], i < N roots, N <= i < 2N weights.
+std::vector<double> rys_power_records(const HostTables& h, int n) {
+    const int rows = h.rys_rows[n];
+    const int nk = rows - 4;
+    std::vector<double> out(static_cast<std::size_t>(nk) * 10 * n, 0.0);
+    for (int k = 0; k < nk; ++k) {
+        for (int i = 0; i < 2 * n; ++i) {
+            const std::vector<double>& src = i < n ? h.rys_roots[n] : h.rys_weights[n];
+            const int col = i < n ? i : i - n;
+            long double f[5];
+            for (int r = 0; r < 5; ++r) f[r] = src[static_cast<std::size_t>(k + r) * n + col];
+            const long double d1 = f[1] - f[0];
+            const long double d2 = (f[2] - 2 * f[1] + f[0]) / 2;
+            const long double d3 = (f[3] - 3 * f[2] + 3 * f[1] - f[0]) / 6;
+            const long double d4 = (f[4] - 4 * f[3] + 6 * f[2] - 4 * f[1] + f[0]) / 24;
+            const long double c[5] = {f[0], d1 - d2 + 2 * d3 - 6 * d4, d2 - 3 * d3 + 11 * d4, d3 - 6 * d4, d4};
+            for (int j = 0; j < 5; ++j) out[(static_cast<std::size_t>(k) * 5 + j) * 2 * n + i] = static_cast<double>(c[j]);
+        }
+    }
+    return out;
+}
+
 int sm_count() {
     static int n = 0;
     if (n == 0) {
@@ -249,12 +277,9 @@ void ensure_device_tables() {
     DevTables t{};
     t.boys = upload(h.boys);
     for (int n = 1; n <= kMaxRoots; ++n) {
-        t.rys_r[n] = upload(h.rys_roots[n]);
-        t.rys_w[n] = upload(h.rys_weights[n]);
-        std::vector<float> r32(h.rys_roots[n].begin(), h.rys_roots[n].end());
-        std::vector<float> w32(h.rys_weights[n].begin(), h.rys_weights[n].end());
-        t.rys_r32[n] = upload(r32);
-        t.rys_w32[n] = upload(w32);
+        const std::vector<double> rec = rys_power_records(h, n);
+        t.rys_h[n] = upload(rec);
+        t.rys_h32[n] = upload(std::vector<float>(rec.begin(), rec.end()));
         t.tmax[n] = h.rys_tmax[n];
         for (int i = 0; i < n; ++i) {
             t.h2[n][i] = h.herm_root2[n][i];
@@ -344,7 +369,21 @@ bool launch_eri_jk_fast(const PlanView& pv, const ClassLaunch& cl, bool fp32, in
     if (idx < 0) return false;
     if (cl.tile_end <= cl.tile_begin) return true;
     const int ntiles = cl.tile_end - cl.tile_begin;
-    if (grid <= 0) grid = sm_count() * 8;
+    // One resident wave of persistent CTAs (a second partial wave would
+    // leave most SMs idle while it runs).
+    static int resident[TLNO_FAST_COUNT][2] = {};
+    int& nb = resident[idx][fp32 ? 1 : 0];
+    if (nb == 0) {
+        switch (idx) {
+#define TLNO_FAST_OCC(id, a, b, c, d) \
+    case id: nb = fast_blocks_per_sm_##id(fp32); break;
+            TLNO_FAST_CLASSES(TLNO_FAST_OCC)
+#undef TLNO_FAST_OCC
+            default: nb = 1;
+        }
+    }
+    const int wave = sm_count() * nb;
+    grid = (grid <= 0) ? wave : std::min(grid, wave);
     grid = std::min(grid, ntiles);
     switch (idx) {
 #define TLNO_FAST_CASE(id, a, b, c, d) \
