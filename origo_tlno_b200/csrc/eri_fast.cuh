@@ -76,7 +76,7 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
     return true;
 }
 
-constexpr int kMaxAccPerSlice = 48;
+constexpr int kMaxAccPerSlice = 64;
 
 __host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
     int t = 1;

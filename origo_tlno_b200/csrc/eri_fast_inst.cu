@@ -147,6 +147,17 @@ namespace tlno_gpu {
 #define TLNO_FAST_IF_18(x)
 #endif
 
+#if TLNO_FAST_ID == 19
+#define TLNO_FAST_IF_19(x) x
+#else
+#define TLNO_FAST_IF_19(x)
+#endif
+#if TLNO_FAST_ID == 20
+#define TLNO_FAST_IF_20(x) x
+#else
+#define TLNO_FAST_IF_20(x)
+#endif
+
 TLNO_FAST_CLASSES(TLNO_FAST_SELECT)
 
 }  // namespace tlno_gpu

@@ -1,8 +1,7 @@
 // Classes with a compile-time ERI kernel (la >= lb, lc >= ld, bra class
-// index >= ket class index): every class with all shells up to d except
-// (dd|dp) and (dd|dd), which take the warp-per-quartet kernel.  Each class is
-// compiled in its own translation unit (eri_fast_inst.cu with
-// -DTLNO_FAST_ID=<index>).
+// index >= ket class index): every class whose shells are at most d.  Higher
+// classes take the warp-per-quartet kernel.  Each class is compiled in its
+// own translation unit (eri_fast_inst.cu with -DTLNO_FAST_ID=<index>).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -26,9 +25,11 @@
     X(15, 2, 2, 0, 0)        \
     X(16, 2, 2, 1, 0)        \
     X(17, 2, 2, 1, 1)        \
-    X(18, 2, 2, 2, 0)
+    X(18, 2, 2, 2, 0)        \
+    X(19, 2, 2, 2, 1)        \
+    X(20, 2, 2, 2, 2)
 
-#define TLNO_FAST_COUNT 19
+#define TLNO_FAST_COUNT 21
 
 namespace tlno_gpu {
 namespace dev {
