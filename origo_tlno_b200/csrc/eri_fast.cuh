@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         const int i = bd.ilocal0 + grp;
         const int j = kb * 32 + lane;
         const int bra = bd.bra0 + (has_bra ? grp : 0);
-        bool active = has_bra && j < bd.nket && !(cl.same && j > i);
+        bool active = has_bra && j < bd.nket && !(cl.same && bd.koff + j > i);
         const int ket = bd.ket0 + (active ? j : 0);
         if (active) {
             const double qq = __ldg(pv.pair_Q + bra) * __ldg(pv.pair_Q + ket);

@@ -350,7 +350,7 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
         for (int jj = warp; jj < cl.bk; jj += warps) {
             const int j = kb * cl.bk + jj;
             if (j >= bd.nket) break;
-            if (cl.same && j > i) break;
+            if (cl.same && bd.koff + j > i) break;
             const int ket = bd.ket0 + j;
             const double qq = qi * pv.pair_Q[ket];
             if (!(qq >= cl.tau)) break;  // kets sorted by Q

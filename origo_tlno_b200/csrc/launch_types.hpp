@@ -27,15 +27,16 @@ struct PlanView {
     const int* mol_M;
 };
 
-// One bra block of a quartet-class schedule: up to `nbra` consecutive bra
-// pairs (sorted by Schwarz bound) against the ket list of the same molecule.
+// One block of a quartet-class schedule: up to `nbra` consecutive bra pairs
+// against one segment of the ket class list of the same molecule (the kets
+// of a segment share their primitive count and are sorted by Schwarz bound).
 struct BlockDesc {
     int bra0;      // first bra pair (global sorted index)
     int nbra;      // bras in this block
-    int ket0;      // first pair of the ket class list of this molecule
-    int nket;      // length of that list
+    int ket0;      // first pair of the ket segment (global sorted index)
+    int nket;      // length of the segment
     int ilocal0;   // position of bra0 inside its own class list (triangle test)
-    int pad;
+    int koff;      // position of the segment inside the ket class list
 };
 
 // Quartet class and the schedule of one launch.

@@ -224,8 +224,13 @@ MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s) {
         if (tau > 0.0 && !(mp.Q_canonical[t] * mp.Qmax >= tau)) continue;
         keep.push_back(t);
     }
+    // Inside a class, pairs are grouped by primitive count (a tile of kets
+    // then runs one primitive loop length on every lane) and sorted by Q
+    // descending inside a group (the kets that pass the bound for a bra
+    // form a prefix of every group).
     std::stable_sort(keep.begin(), keep.end(), [&](long long l, long long r) {
         if (mp.cls[l] != mp.cls[r]) return mp.cls[l] < mp.cls[r];
+        if (mp.nprim[l] != mp.nprim[r]) return mp.nprim[l] < mp.nprim[r];
         return mp.Q_canonical[l] > mp.Q_canonical[r];
     });
     MolPairs out;
@@ -368,43 +373,54 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                 const int nX = mp.cls_count[X], nY = mp.cls_count[Y];
                 if (nX == 0 || nY == 0) continue;
                 const int bx0 = gbeg[m][X], by0 = gbeg[m][Y];
-                // ket nprim prefix sums for the primitive-quartet count
-                std::vector<long long> kp(nY + 1, 0);
-                for (int j = 0; j < nY; ++j) kp[j + 1] = kp[j] + plan.pair_nprim[by0 + j];
+                // ket segments of equal primitive count
+                std::vector<int> seg{0};
+                for (int j = 1; j < nY; ++j)
+                    if (plan.pair_nprim[by0 + j] != plan.pair_nprim[by0 + j - 1]) seg.push_back(j);
+                seg.push_back(nY);
                 const double* qk = plan.pair_Q.data() + by0;
-                auto ket_extent = [&](double qi) {
-                    if (tau <= 0.0) return nY;
-                    // first j with qi * qk[j] < tau (qk descending)
-                    int lo = 0, hi = nY;
-                    while (lo < hi) {
-                        const int mid = (lo + hi) / 2;
-                        if (qi * qk[mid] >= tau) lo = mid + 1; else hi = mid;
+                // kets of segment [s0, s1) with qi * Q >= tau, and (diagonal
+                // class) local index <= i
+                auto seg_extent = [&](double qi, int s0, int s1, int i) {
+                    int lo = s0, hi = s1;
+                    if (tau > 0.0) {
+                        while (lo < hi) {
+                            const int mid = (lo + hi) / 2;
+                            if (qi * qk[mid] >= tau) lo = mid + 1; else hi = mid;
+                        }
+                    } else {
+                        lo = s1;
                     }
-                    return lo;
+                    int e = lo - s0;
+                    if (X == Y) e = std::min(e, i + 1 - s0);
+                    return std::max(e, 0);
                 };
                 for (int i0 = 0; i0 < nX; i0 += cs.bb) {
                     const int nbra = std::min(cs.bb, nX - i0);
-                    int ext = ket_extent(plan.pair_Q[bx0 + i0]);
-                    if (X == Y) ext = std::min(ext, i0 + nbra);
-                    // exact statistics per bra
-                    for (int w = 0; w < nbra; ++w) {
-                        const int i = i0 + w;
-                        int e = ket_extent(plan.pair_Q[bx0 + i]);
-                        if (X == Y) e = std::min(e, i + 1);
-                        if (e <= 0) continue;
-                        cs.quartets += e;
-                        cs.prim_quartets += static_cast<long long>(plan.pair_nprim[bx0 + i]) * kp[e];
+                    for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
+                        const int s0 = seg[sg], s1 = seg[sg + 1];
+                        const long long npk = plan.pair_nprim[by0 + s0];
+                        int ext = 0;
+                        // exact statistics per bra
+                        for (int w = 0; w < nbra; ++w) {
+                            const int i = i0 + w;
+                            const int e = seg_extent(plan.pair_Q[bx0 + i], s0, s1, i);
+                            ext = std::max(ext, e);
+                            cs.quartets += e;
+                            cs.prim_quartets += static_cast<long long>(plan.pair_nprim[bx0 + i]) * npk * e;
+                        }
+                        const int nt = (ext + cs.bk - 1) / cs.bk;
+                        if (nt <= 0) continue;
+                        dev::BlockDesc bd{};
+                        bd.bra0 = bx0 + i0;
+                        bd.nbra = nbra;
+                        bd.ket0 = by0 + s0;
+                        bd.nket = s1 - s0;
+                        bd.ilocal0 = i0;
+                        bd.koff = s0;
+                        cs.blocks.push_back(bd);
+                        cs.prefix.push_back(cs.prefix.back() + nt);
                     }
-                    const int nt = (ext + cs.bk - 1) / cs.bk;
-                    if (nt <= 0) continue;
-                    dev::BlockDesc bd{};
-                    bd.bra0 = bx0 + i0;
-                    bd.nbra = nbra;
-                    bd.ket0 = by0;
-                    bd.nket = nY;
-                    bd.ilocal0 = i0;
-                    cs.blocks.push_back(bd);
-                    cs.prefix.push_back(cs.prefix.back() + nt);
                 }
             }
             cs.n_tiles = cs.prefix.back();
