@@ -353,8 +353,8 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
             if (cl.same && bd.koff + j > i) break;
             const int ket = bd.ket0 + j;
             const double qq = qi * pv.pair_Q[ket];
-            if (!(qq >= cl.tau)) break;  // kets sorted by Q
-            if (cl.prec_mode == 1 && !(qq >= thr)) break;
+            if (!(qq >= cl.tau)) continue;
+            if (cl.prec_mode == 1 && !(qq >= thr)) continue;
             if (cl.prec_mode == 2 && qq >= thr) continue;
             generic_quartet<R, kJK>(pv, cl, lay, wsm, lane, bra, ket, 0);
         }

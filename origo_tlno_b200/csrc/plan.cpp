@@ -24,6 +24,17 @@
 namespace tlno_gpu {
 
 namespace {
+// Schwarz bucket of a pair: floor(-log2 Q), so bucket k holds
+// Q in (2^-(k+1), 2^-k]; larger Q first.
+int Q_bucket(double q) {
+    if (!(q > 0.0)) return 1 << 20;
+    int e = 0;
+    const double m = std::frexp(q, &e);  // q = m 2^e, m in [0.5, 1)
+    return (m == 0.5) ? 1 - e : -e;      // q == 2^(e-1) belongs to bucket 1-e
+}
+}  // namespace
+
+namespace {
 
 template <class T>
 void upload_vec(DeviceBuffer& buf, const std::vector<T>& v, cudaStream_t s) {
@@ -225,13 +236,19 @@ MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s) {
         keep.push_back(t);
     }
     // Inside a class, pairs are grouped by primitive count (a tile of kets
-    // then runs one primitive loop length on every lane) and sorted by Q
-    // descending inside a group (the kets that pass the bound for a bra
-    // form a prefix of every group).
+    // then runs one primitive loop length on every lane), then by Schwarz
+    // bucket floor(-log2 Q) (the kets that can pass the bound for a bra form
+    // a prefix of whole buckets), and inside a bucket by shell indices, so
+    // that neighbouring lanes read and update neighbouring density and J/K
+    // elements.
+    auto bucket = [&](long long t) { return Q_bucket(mp.Q_canonical[t]); };
     std::stable_sort(keep.begin(), keep.end(), [&](long long l, long long r) {
         if (mp.cls[l] != mp.cls[r]) return mp.cls[l] < mp.cls[r];
         if (mp.nprim[l] != mp.nprim[r]) return mp.nprim[l] < mp.nprim[r];
-        return mp.Q_canonical[l] > mp.Q_canonical[r];
+        const int bl = bucket(l), br = bucket(r);
+        if (bl != br) return bl < br;
+        if (mp.A[l] != mp.A[r]) return mp.A[l] < mp.A[r];
+        return mp.B[l] < mp.B[r];
     });
     MolPairs out;
     out.Q_canonical = std::move(mp.Q_canonical);
@@ -379,22 +396,83 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                     if (plan.pair_nprim[by0 + j] != plan.pair_nprim[by0 + j - 1]) seg.push_back(j);
                 seg.push_back(nY);
                 const double* qk = plan.pair_Q.data() + by0;
-                // kets of segment [s0, s1) with qi * Q >= tau, and (diagonal
-                // class) local index <= i
+                // Per segment: Q sorted descending (exact quartet counts) and,
+                // per position, the largest Q of its bucket (non-increasing
+                // along the segment) for the schedule extent.
+                std::vector<double> qsorted(qk, qk + nY), bmax(nY);
+                for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
+                    const int s0 = seg[sg], s1 = seg[sg + 1];
+                    std::sort(qsorted.begin() + s0, qsorted.begin() + s1, std::greater<double>());
+                    for (int j = s0; j < s1;) {
+                        int e = j;
+                        double mx = 0.0;
+                        const int bk = Q_bucket(qk[j]);
+                        while (e < s1 && Q_bucket(qk[e]) == bk) mx = std::max(mx, qk[e++]);
+                        for (int t = j; t < e; ++t) bmax[t] = mx;
+                        j = e;
+                    }
+                }
+                // Tile extent of segment [s0, s1) for a bra of bound qi: the
+                // whole buckets that may hold a passing ket (on the diagonal
+                // class only local index <= i).
                 auto seg_extent = [&](double qi, int s0, int s1, int i) {
-                    int lo = s0, hi = s1;
+                    int lo = s1;
                     if (tau > 0.0) {
+                        lo = s0;
+                        int hi = s1;
                         while (lo < hi) {
                             const int mid = (lo + hi) / 2;
-                            if (qi * qk[mid] >= tau) lo = mid + 1; else hi = mid;
+                            if (qi * bmax[mid] >= tau) lo = mid + 1; else hi = mid;
                         }
-                    } else {
-                        lo = s1;
                     }
                     int e = lo - s0;
                     if (X == Y) e = std::min(e, i + 1 - s0);
                     return std::max(e, 0);
                 };
+                // passing kets of segment [s0, s1) for a bra of bound qi
+                auto seg_count = [&](double qi, int s0, int s1) {
+                    if (tau <= 0.0) return s1 - s0;
+                    int a = s0, b = s1;
+                    while (a < b) {
+                        const int mid = (a + b) / 2;
+                        if (qi * qsorted[mid] >= tau) a = mid + 1; else b = mid;
+                    }
+                    return a - s0;
+                };
+                // Exact surviving quartets and primitive quartets.  Off the
+                // diagonal every (bra, ket) pair counts; on the diagonal class
+                // (one list, j <= i) a ket segment before the bra's segment
+                // counts fully and the bra's own segment holds
+                // (ordered pairs + self pairs) / 2.
+                {
+                    std::vector<int> seg_of(nX);
+                    if (X == Y)
+                        for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg)
+                            for (int j = seg[sg]; j < seg[sg + 1]; ++j) seg_of[j] = static_cast<int>(sg);
+                    std::vector<long long> own_ordered(seg.size(), 0), own_self(seg.size(), 0);
+                    for (int i = 0; i < nX; ++i) {
+                        const double qi = plan.pair_Q[bx0 + i];
+                        const long long npb = plan.pair_nprim[bx0 + i];
+                        for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
+                            if (X == Y && static_cast<int>(sg) > seg_of[i]) break;
+                            const int c = seg_count(qi, seg[sg], seg[sg + 1]);
+                            if (X == Y && static_cast<int>(sg) == seg_of[i]) {
+                                own_ordered[sg] += c;
+                                if (tau <= 0.0 || qi * qi >= tau) own_self[sg] += 1;
+                                continue;
+                            }
+                            cs.quartets += c;
+                            cs.prim_quartets += npb * plan.pair_nprim[by0 + seg[sg]] * c;
+                        }
+                    }
+                    if (X == Y)
+                        for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
+                            const long long n = (own_ordered[sg] + own_self[sg]) / 2;
+                            const long long np = plan.pair_nprim[by0 + seg[sg]];
+                            cs.quartets += n;
+                            cs.prim_quartets += np * np * n;
+                        }
+                }
                 for (int i0 = 0; i0 < nX; i0 += cs.bb) {
                     const int nbra = std::min(cs.bb, nX - i0);
                     for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
@@ -404,10 +482,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                         // exact statistics per bra
                         for (int w = 0; w < nbra; ++w) {
                             const int i = i0 + w;
-                            const int e = seg_extent(plan.pair_Q[bx0 + i], s0, s1, i);
-                            ext = std::max(ext, e);
-                            cs.quartets += e;
-                            cs.prim_quartets += static_cast<long long>(plan.pair_nprim[bx0 + i]) * npk * e;
+                            ext = std::max(ext, seg_extent(plan.pair_Q[bx0 + i], s0, s1, i));
                         }
                         const int nt = (ext + cs.bk - 1) / cs.bk;
                         if (nt <= 0) continue;
