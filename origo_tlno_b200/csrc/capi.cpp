@@ -104,12 +104,14 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
                 double* d_dmax, cudaStream_t s) {
     TLNO_CUDA(cudaMemsetAsync(dJ, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(dK, 0, sizeof(double) * total, s));
+    TLNO_CUDA(cudaMemsetAsync(plan.d_counters.ptr, 0, sizeof(int) * 2 * plan.combos.size(), s));
     if (mixed) launch_absmax(dD, total, d_dmax, s);
     const dev::PlanView pv = plan.view();
     int sms = 0, devid = 0;
     TLNO_CUDA(cudaGetDevice(&devid));
     TLNO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devid));
-    for (ComboSchedule& cs : plan.combos) {
+    for (std::size_t ci = 0; ci < plan.combos.size(); ++ci) {
+        ComboSchedule& cs = plan.combos[ci];
         dev::ClassLaunch cl{};
         cl.la = cs.la; cl.lb = cs.lb; cl.lc = cs.lc; cl.ld = cs.ld;
         cl.same = (cs.X == cs.Y);
@@ -133,6 +135,7 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
         const int passes = mixed ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
             cl.prec_mode = mixed ? (pass + 1) : 0;
+            cl.counter = plan.d_counters.as<int>() + 2 * ci + pass;
             const bool fp32 = mixed && pass == 1;
             if (cs.fast) {
                 launch_eri_jk_fast(pv, cl, fp32, grid, s);
@@ -689,7 +692,9 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int re
         TLNO_CUDA(cudaEventCreate(&e0));
         TLNO_CUDA(cudaEventCreate(&e1));
         const dev::PlanView pv = plan.view();
+        cl.counter = plan.d_counters.as<int>() + 2 * combo_index;
         auto run = [&] {
+            TLNO_CUDA(cudaMemsetAsync(cl.counter, 0, sizeof(int), s));
             if (cs.fast) launch_eri_jk_fast(pv, cl, fp32 != 0, grid, s);
             else launch_eri_jk_generic(pv, cl, fp32 != 0, ctx->tune.generic_warps, grid, s);
         };

@@ -2,9 +2,9 @@
 // (thread per contracted quartet, the quartet's work sliced over TPQ warps).
 //
 // Tile: a group of TPQ warps takes one bra shell pair and 32 consecutive ket
-// shell pairs of the same class (one quartet per lane); a CTA holds BBQ
-// groups on consecutive bra pairs.  Kets are sorted by Schwarz bound, so the
-// quartets of a tile that fail the bound form a suffix.
+// shell pairs of one primitive-count segment of the same class (one quartet
+// per lane); a CTA holds BBQ independent groups, each pulling chunks of
+// tiles from a launch counter.
 //
 // Phase 1 (registers): every thread of a quartet evaluates the primitive
 // loop (Rys roots/weights, 2-D VRR) and accumulates its own slice of the
@@ -77,6 +77,7 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
 }
 
 constexpr int kMaxAccPerSlice = 64;
+constexpr int kTileChunk = 4;  // tiles per dynamic-schedule fetch
 
 __host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
     int t = 1;
@@ -294,6 +295,21 @@ __device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, i
     }
 }
 
+// Barrier and OR-vote over the TPQ warps of one group (named barrier
+// 1 + group, so the groups of a CTA run independent control flow).
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ bool group_any(bool pred, int id, int nthreads) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\tselp.s32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(pred ? 1 : 0), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 template <typename R, int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     eri_fast_jk_kernel(PlanView pv, ClassLaunch cl) {
@@ -310,16 +326,41 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     else
         ks = fast_smem + (grp * 32 + lane) * S::LANE_STRIDE;
     const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
+    const int bar_id = 1 + grp, bar_n = 32 * S::TPQ;
+    __shared__ int s_chunk[S::BBQ];
+    const int ntiles = cl.tile_end - cl.tile_begin;
 
-    for (int tile = cl.tile_begin + blockIdx.x; tile < cl.tile_end; tile += gridDim.x) {
-        const int b = find_block(cl.tile_prefix, cl.n_blocks, tile);
+    // Dynamic schedule: every warp group takes kTileChunk consecutive tiles
+    // (one bra pair x 32 kets each) from the launch counter, so all groups
+    // work inside one moving window of the schedule and the density, J and
+    // K rows of the bras in flight stay in L2.  The first tile's block comes
+    // from a binary search, the next ones from walking the prefix forward.
+    for (;;) {
+        int c0;
+        if constexpr (S::TPQ == 1) {
+            c0 = (lane == 0) ? atomicAdd(cl.counter, kTileChunk) : 0;
+            c0 = __shfl_sync(0xffffffffu, c0, 0);
+        } else {
+            if (g == 0 && lane == 0) s_chunk[grp] = atomicAdd(cl.counter, kTileChunk);
+            group_sync(bar_id, bar_n);
+            c0 = s_chunk[grp];
+            group_sync(bar_id, bar_n);
+        }
+        if (c0 >= ntiles) break;
+        const int c1 = min(c0 + kTileChunk, ntiles);
+        int b = find_block(cl.tile_prefix, cl.n_blocks, cl.tile_begin + c0);
+        int next = __ldg(cl.tile_prefix + b + 1);
+    for (int tile = cl.tile_begin + c0; tile < cl.tile_begin + c1; ++tile) {
+        while (tile >= next) {
+            ++b;
+            next = __ldg(cl.tile_prefix + b + 1);
+        }
         const int kb = tile - __ldg(cl.tile_prefix + b);
         const BlockDesc bd = cl.blocks[b];
-        const bool has_bra = grp < bd.nbra;
-        const int i = bd.ilocal0 + grp;
+        const int i = bd.ilocal0;  // one bra per block
         const int j = kb * 32 + lane;
-        const int bra = bd.bra0 + (has_bra ? grp : 0);
-        bool active = has_bra && j < bd.nket && !(cl.same && bd.koff + j > i);
+        const int bra = bd.bra0;
+        bool active = j < bd.nket && !(cl.same && bd.koff + j > i);
         const int ket = bd.ket0 + (active ? j : 0);
         if (active) {
             const double qq = __ldg(pv.pair_Q + bra) * __ldg(pv.pair_Q + ket);
@@ -329,7 +370,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         }
         bool any;
         if constexpr (S::TPQ > 1)
-            any = __syncthreads_or(active) != 0;
+            any = group_any(active, bar_id, bar_n);
         else
             any = __any_sync(0xffffffffu, active);
         if (!any) continue;
@@ -346,7 +387,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         }
 
         fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, ks);
-        if constexpr (S::TPQ > 1) __syncthreads();
+        if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
 
         // ---- phase 3: bra transfer + projection per owned ket column, digestion ----
         const int mol = pv.pair_mol ? __ldg(pv.pair_mol + bra) : 0;
@@ -452,10 +493,11 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                 double s = fj * jab[e];
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0 && has_bra && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
+                if (lane == 0 && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
             }
         }
-        if constexpr (S::TPQ > 1) __syncthreads();
+        if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
+    }
     }
 }
 
@@ -463,7 +505,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_warps() { return FastShape<LA, LB, LC, LD>::WARPS; }
 template <int LA, int LB, int LC, int LD>
-constexpr int fast_bras() { return FastShape<LA, LB, LC, LD>::BBQ; }
+constexpr int fast_bras() { return 1; }
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_smem_bytes() { return FastShape<LA, LB, LC, LD>::SMEM_DOUBLES * 8; }
 

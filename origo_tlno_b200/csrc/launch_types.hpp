@@ -48,6 +48,7 @@ struct ClassLaunch {
     const int* tile_prefix;       // per block: first tile index (n_blocks + 1)
     int n_blocks;
     int tile_begin, tile_end;     // tile range of this launch
+    int* counter;                 // dynamic-schedule counter, zero at launch (compile-time kernels)
     double tau;                   // Schwarz threshold
     // Precision split: mode 0 = every quartet; 1 = quartets with
     // Q_ab Q_cd max|D| >= tau_mix only (FP64 part); 2 = the complement.

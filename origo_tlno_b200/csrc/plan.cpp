@@ -509,6 +509,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
             plan.combos.push_back(std::move(cs));
         }
     }
+    plan.d_counters.alloc(sizeof(int) * 2 * std::max<std::size_t>(plan.combos.size(), 1));
     TLNO_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -55,6 +55,7 @@ public:
     std::vector<int> pair_A, pair_B, pair_nprim, pair_prim_off, pair_mol;
     std::vector<double> pair_Q;
     std::vector<ComboSchedule> combos;
+    DeviceBuffer d_counters;  // dynamic-schedule counters, 2 per combo (FP64 and FP32 pass)
     DeviceBuffer d_shell_xyz, d_shell_L, d_shell_sph;
     DeviceBuffer d_pair_A, d_pair_B, d_pair_prim_off, d_pair_nprim, d_pair_Q, d_pair_mol;
     DeviceBuffer d_prim, d_mol_mat_off, d_mol_M;
