@@ -135,9 +135,9 @@ def _reference_sample(name, seconds_target=15.0):
     from origo_tlno_b200 import engine as E
     from oracle import ref
     if name in ("cfg4",) or name.startswith("water"):
-        sample_mol = MOL.water_cluster(8, seed=5)
+        sample_mol = MOL.water_cluster(40, seed=5)
         tau = 1e-11
-        desc = "8-water sub-cluster of the cfg4 recipe (M=192), Schwarz 1e-11, one J+K build"
+        desc = "40-water sub-cluster of the cfg4 recipe (M=960), Schwarz 1e-11, one J+K build"
     elif name == "cfg2":
         sample_mol = MOL.cfg1()
         tau = 1e-12
@@ -205,6 +205,19 @@ def _count_quartets(mol, tau):
                 hi = mid
         total += lo
     return total
+
+
+def _profiled_traffic(workload, tag):
+    """DRAM bytes per launch of class `tag` on `workload` from the committed
+    ncu summary (profiles/dram_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            table = json.load(f)
+    except (OSError, ValueError):
+        return None
+    v = table.get(workload, {}).get(tag)
+    return float(v) if v is not None else None
 
 
 def run_native(args):
@@ -300,14 +313,18 @@ def run_native(args):
     for i, cb in enumerate(combos):
         if cb["n_tiles"] == 0:
             continue
-        t = ctx.time_combo(i, fp32=False, reps=2)
+        t = ctx.time_combo(i, fp32=False, reps=1)
         timings.append((t, i, cb))
     timings.sort(key=lambda x: -x[0])
     tdom, idom, cdom = timings[0]
     peak = E.fma_peak_tflops(False, device=local)
     achieved = cdom["flops"] / (tdom * 1e-3) / 1e12
-    launches_fp64 = sum(1 for cb in combos if cb["n_tiles"] > 0) + 4
-    launches = 2 * sum(1 for cb in combos if cb["n_tiles"] > 0) + 5
+    dom_tag = f"({cdom['la']}{cdom['lb']}|{cdom['lc']}{cdom['ld']})"
+    traffic = _profiled_traffic(args.config, dom_tag)
+    # kernels per build: one per class combination and precision pass, the
+    # max|D| reduction (mixed) and the two final symmetrisations
+    n_cls = sum(1 for cb in combos if cb["n_tiles"] > 0)
+    launches = 2 * n_cls + 3
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -336,10 +353,14 @@ def run_native(args):
         "mixed_speedup_vs_fp64": t64 / tmx,
         "accuracy": {"abs_dE_Eh": abs(dE), "max_abs_dJ": dJ, "max_abs_dK": dK},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak else None, "traffic": None,
-                     "kernel": f"eri class ({cdom['la']}{cdom['lb']}|{cdom['lc']}{cdom['ld']}) "
-                               f"{'thread-per-quartet' if cdom['fast'] else 'warp-per-quartet'}",
-                     "peak_source": "measured DFMA-chain probe (tlno_gpu_fma_peak) on this GPU"},
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "kernel": f"eri_fast_jk_kernel<double> class {dom_tag}" if cdom["fast"] else
+                               f"eri_generic_jk_kernel<double> class {dom_tag}",
+                     "launch_ms": tdom,
+                     "peak_source": "of measured: DFMA-chain probe (tlno_gpu_fma_peak) on this GPU; "
+                                    "MEASURED_PEAKS.json holds no FP64 figure",
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu "
+                                       "capture of the same class and workload (profiles/)"},
         "e2e": e2e, "gpu_launches": launches * steps,
         "clocks": clocks, "wall_s_timed": t_wall,
         "cpu_baseline": cpu,
@@ -355,7 +376,7 @@ def run_native(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--config", default="cfg4")

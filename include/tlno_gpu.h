@@ -206,9 +206,11 @@ int tlno_gpu_batch_graph_launch(tlno_gpu_batch* b);
 int tlno_gpu_batch_synchronize(tlno_gpu_batch* b);
 void* tlno_gpu_batch_stream(tlno_gpu_batch* b);
 
-/* Tuning of the kernel schedule (autotuner output): thread-per-quartet CTA
- * bra pairs, generic-kernel ket tile, generic warps per CTA, persistent
- * grid multiplier, and a per-class-combination generic override. */
+/* Tuning of the kernel schedule: fast_bb is accepted (1..4) and ignored
+ * (the compile-time kernels take one bra pair per tile and size their grid
+ * from the occupancy calculator, capped by grid_mult x SMs);
+ * generic-kernel ket tile, generic warps per CTA, persistent grid
+ * multiplier; and a per-class-combination generic override. */
 typedef struct {
     int fast_bb;
     int generic_bk;

@@ -1,0 +1,76 @@
+"""Per-class statistics and timings of the direct J/K build.
+
+Plans a synthetic workload and, for every quartet class combination (or the
+selected ones), prints one JSON line: surviving contracted and primitive
+quartets, the flop model, the kernel (compile-time or warp-per-quartet) and
+the CUDA-event time of one class launch in FP64, FP32 and without J/K
+digestion.  With --once it only launches the selected classes one time each
+(a target for a profiler run).
+
+    python -m origo_tlno_b200.classprof cfg4 --classes "10|00" --once
+    python -m origo_tlno_b200.classprof water60 --reps 3 --fp32
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+from . import engine as E
+from . import molecules as M
+
+
+def workload(name: str):
+    """Molecule and Schwarz threshold of a named synthetic workload."""
+    if name.startswith("water"):
+        return M.water_cluster(int(name[5:]), seed=5), 1e-11
+    mol = getattr(M, name)()
+    return mol, (1e-11 if name == "cfg4" else 1e-12)
+
+
+def tag(c) -> str:
+    return f"{c['la']}{c['lb']}|{c['lc']}{c['ld']}"
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("workload", help="cfg0..cfg4 or waterN")
+    ap.add_argument("--classes", default="", help='comma-separated class tags such as "10|00,11|10"')
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--fp32", action="store_true", help="also time the FP32 kernel of each class")
+    ap.add_argument("--eri-only", action="store_true", help="also time the class without J/K digestion")
+    ap.add_argument("--once", action="store_true", help="launch each selected class once, no timing loop")
+    ap.add_argument("--plan-only", action="store_true")
+    a = ap.parse_args(argv)
+
+    mol, tau = workload(a.workload)
+    t0 = time.time()
+    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=tau))
+    prof = ctx.profile()
+    prof["plan_s"] = time.time() - t0
+    prof["workload"] = a.workload
+    print(json.dumps(prof), flush=True)
+    want = {t.strip() for t in a.classes.split(",") if t.strip()}
+    for i, c in enumerate(ctx.combos()):
+        if want and tag(c) not in want:
+            continue
+        row = {"index": i, "class": tag(c), "kernel": "compile-time" if c["fast"] else "warp-per-quartet",
+               "tiles": c["n_tiles"], "quartets": c["quartets"], "prim_quartets": c["prim_quartets"],
+               "flops_model": c["flops"]}
+        if not a.plan_only:
+            reps = 0 if a.once else a.reps
+            ms = ctx.time_combo(i, reps=reps)
+            row["ms_fp64"] = ms
+            if not a.once:
+                row["tflops_model"] = c["flops"] / (ms * 1e-3) / 1e12
+                if a.eri_only:
+                    row["ms_fp64_eri_only"] = ctx.time_combo(i, reps=a.reps, want_j=False, want_k=False)
+                if a.fp32:
+                    row["ms_fp32"] = ctx.time_combo(i, fp32=True, reps=a.reps)
+        print(json.dumps(row), flush=True)
+    ctx.close()
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

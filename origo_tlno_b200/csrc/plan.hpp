@@ -12,7 +12,7 @@
 namespace tlno_gpu {
 
 struct Tuning {
-    int fast_bb = 4;        // bra pairs per CTA (warps) of the thread-per-quartet kernels
+    int fast_bb = 4;        // accepted and ignored (compile-time kernels take one bra per tile)
     int generic_bk = 16;    // ket pairs per tile of the warp-per-quartet kernel
     int generic_warps = 0;  // 0 = from shared-memory budget
     int grid_mult = 8;      // CTAs per SM for persistent launches
