@@ -118,6 +118,7 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
         cl.bb = cs.bb;
         cl.bk = cs.bk;
         cl.blocks = cs.d_blocks.as<dev::BlockDesc>();
+        cl.bra_list = cs.d_bra_list.as<int>();
         cl.tile_prefix = cs.d_prefix.as<int>();
         cl.n_blocks = static_cast<int>(cs.blocks.size());
         cl.tile_begin = 0;
@@ -674,6 +675,7 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int re
         cl.same = cs.X == cs.Y;
         cl.bb = cs.bb; cl.bk = cs.bk;
         cl.blocks = cs.d_blocks.as<dev::BlockDesc>();
+        cl.bra_list = cs.d_bra_list.as<int>();
         cl.tile_prefix = cs.d_prefix.as<int>();
         cl.n_blocks = static_cast<int>(cs.blocks.size());
         cl.tile_begin = 0;

@@ -78,6 +78,8 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
 
 constexpr int kMaxAccPerSlice = 64;
 constexpr int kTileChunk = 4;  // tiles per dynamic-schedule fetch
+constexpr int kBraGroup = 8;   // bras per block of the light classes
+constexpr int kMaxCarried = 16;
 
 __host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
     int t = 1;
@@ -104,6 +106,11 @@ struct FastShape {
     // Phase-3 work split: by ket spherical function c when there are enough
     // of them (K[ac], K[bc] complete inside one warp), else by column (c,d).
     static constexpr bool BY_SC = NSC >= TPQ;
+    // Bras per schedule block, all with the same first shell A: a lane's
+    // J[cd], K[ac] and K[ad] sums stay in registers across the block, which
+    // divides those FP64 atomics by the block size.  Only for unsliced
+    // classes whose carried sums are small.
+    static constexpr int GB = (TPQ == 1 && NSA * (NSC + NSD) + NSCD <= kMaxCarried) ? kBraGroup : 1;
     static constexpr int LANE_STRIDE = (NAS * NSCD) | 1;  // odd: conflict-free FP64 rows
     static constexpr int SMEM_DOUBLES = TPQ == 1 ? 0 : BBQ * 32 * LANE_STRIDE;
 };
@@ -357,146 +364,221 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         }
         const int kb = tile - __ldg(cl.tile_prefix + b);
         const BlockDesc bd = cl.blocks[b];
-        const int i = bd.ilocal0;  // one bra per block
         const int j = kb * 32 + lane;
-        const int bra = bd.bra0;
-        bool active = j < bd.nket && !(cl.same && bd.koff + j > i);
-        const int ket = bd.ket0 + (active ? j : 0);
-        if (active) {
-            const double qq = __ldg(pv.pair_Q + bra) * __ldg(pv.pair_Q + ket);
-            active = qq >= cl.tau;
-            if (cl.prec_mode == 1) active = active && qq >= thr;
-            if (cl.prec_mode == 2) active = active && !(qq >= thr);
-        }
-        bool any;
-        if constexpr (S::TPQ > 1)
-            any = group_any(active, bar_id, bar_n);
-        else
-            any = __any_sync(0xffffffffu, active);
-        if (!any) continue;
+        const bool lane_ok = j < bd.nket;
+        const int ket = bd.ket0 + (lane_ok ? j : 0);
 
-        const int A = __ldg(pv.pair_A + bra), B = __ldg(pv.pair_B + bra);
+        // ket side, once per tile
         const int C = __ldg(pv.pair_A + ket), D = __ldg(pv.pair_B + ket);
+        const double qket = __ldg(pv.pair_Q + ket);
         QuartetGeom q;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            q.A[k] = __ldg(pv.shell_xyz + 3 * A + k);
             q.C[k] = __ldg(pv.shell_xyz + 3 * C + k);
-            q.AB[k] = q.A[k] - __ldg(pv.shell_xyz + 3 * B + k);
             q.CD[k] = q.C[k] - __ldg(pv.shell_xyz + 3 * D + k);
         }
-
-        fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, ks);
-        if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
-
-        // ---- phase 3: bra transfer + projection per owned ket column, digestion ----
-        const int mol = pv.pair_mol ? __ldg(pv.pair_mol + bra) : 0;
+        const int mol = pv.pair_mol ? __ldg(pv.pair_mol + ket) : 0;
         const int M = pv.mol_M ? __ldg(pv.mol_M + mol) : cl.M;
         const long long mbase = pv.mol_mat_off ? __ldg(pv.mol_mat_off + mol) : 0;
         const double* Dm = cl.dens + mbase;
         double* Jm = cl.J + mbase;
         double* Km = cl.K + mbase;
-        const int a0 = __ldg(pv.shell_sph + A), b0 = __ldg(pv.shell_sph + B);
-        const int c0 = __ldg(pv.shell_sph + C), d0 = __ldg(pv.shell_sph + D);
-        double f = active ? 1.0 : 0.0;
-        if (A == B) f *= 0.5;
-        if (C == D) f *= 0.5;
-        if (bra == ket) f *= 0.5;
-        const double fj = 4.0 * f, fk = 2.0 * f;
         auto dm = [&](int r, int c) { return __ldg(Dm + (long long)r * M + c); };
+        const int c0 = __ldg(pv.shell_sph + C), d0 = __ldg(pv.shell_sph + D);
 
-        double jab[S::NSAB];
+        // Sums carried across the bras of a block (they share the first
+        // shell A): J[cd], K[ac], K[ad] of this lane's ket.
+        constexpr bool CARRY = S::GB > 1;
+        double jcd[CARRY ? S::NSCD : 1];
+        double kacc[CARRY ? S::NSA : 1][CARRY ? S::NSC : 1];
+        double kadc[CARRY ? S::NSA : 1][CARRY ? S::NSD : 1];
+        if constexpr (CARRY) {
 #pragma unroll
-        for (int e = 0; e < S::NSAB; ++e) jab[e] = 0.0;
-
-        if (active) {
-            double kad[S::NSA][S::NSD], kbd[S::NSB][S::NSD];
+            for (int t = 0; t < S::NSCD; ++t) jcd[t] = 0.0;
 #pragma unroll
-            for (int sd = 0; sd < S::NSD; ++sd) {
+            for (int a = 0; a < S::NSA; ++a) {
 #pragma unroll
-                for (int a = 0; a < S::NSA; ++a) kad[a][sd] = 0.0;
+                for (int c = 0; c < S::NSC; ++c) kacc[a][c] = 0.0;
 #pragma unroll
-                for (int bq = 0; bq < S::NSB; ++bq) kbd[bq][sd] = 0.0;
+                for (int d = 0; d < S::NSD; ++d) kadc[a][d] = 0.0;
             }
-            sfor<S::NSC>([&](auto SC) {
-                constexpr int sc = TLNO_CI(SC);
-                double kac[S::NSA], kbc[S::NSB];
+        }
+        bool touched = false;
+        int a0 = 0;
+
+        for (int ib = 0; ib < S::GB && ib < bd.nbra; ++ib) {
+            const int bra = __ldg(cl.bra_list + bd.bra0 + ib);
+            const int i = bra - bd.xbeg;
+            bool active = lane_ok && !(cl.same && bd.koff + j > i);
+            if (active) {
+                const double qq = __ldg(pv.pair_Q + bra) * qket;
+                active = qq >= cl.tau;
+                if (cl.prec_mode == 1) active = active && qq >= thr;
+                if (cl.prec_mode == 2) active = active && !(qq >= thr);
+            }
+            bool any;
+            if constexpr (S::TPQ > 1)
+                any = group_any(active, bar_id, bar_n);
+            else
+                any = __any_sync(0xffffffffu, active);
+            if (!any) continue;
+            touched = touched || active;
+
+            const int A = __ldg(pv.pair_A + bra), B = __ldg(pv.pair_B + bra);
 #pragma unroll
-                for (int a = 0; a < S::NSA; ++a) kac[a] = 0.0;
+            for (int k = 0; k < 3; ++k) {
+                q.A[k] = __ldg(pv.shell_xyz + 3 * A + k);
+                q.AB[k] = q.A[k] - __ldg(pv.shell_xyz + 3 * B + k);
+            }
+            fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, ks);
+            if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
+
+            // ---- bra transfer + projection per owned ket column, digestion ----
+            a0 = __ldg(pv.shell_sph + A);
+            const int b0 = __ldg(pv.shell_sph + B);
+            double f = active ? 1.0 : 0.0;
+            if (A == B) f *= 0.5;
+            if (C == D) f *= 0.5;
+            if (bra == ket) f *= 0.5;
+            const double fj = 4.0 * f, fk = 2.0 * f;
+
+            double jab[S::NSAB];
 #pragma unroll
-                for (int bq = 0; bq < S::NSB; ++bq) kbc[bq] = 0.0;
-                bool own_sc = false;
-                sfor<S::NSD>([&](auto SD) {
-                    constexpr int sd = TLNO_CI(SD);
-                    constexpr int t = sc * S::NSD + sd;
-                    const bool own = S::BY_SC ? (sc % S::TPQ == g) : (t % S::TPQ == g);
-                    if (!own) return;
-                    own_sc = true;
-                    double V[S::NSAB];
-                    sfor<S::NSA>([&](auto SA) {
-                        sfor<S::NSB>([&](auto SB) {
-                            constexpr int sa = TLNO_CI(SA), sb = TLNO_CI(SB);
-                            V[sa * S::NSB + sb] = pair_transfer<LA, LB, sa, sb, S::OFA>(
-                                q.AB, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
-                        });
-                    });
-                    if (cl.want_j) {
-                        double s = 0.0;
+            for (int e = 0; e < S::NSAB; ++e) jab[e] = 0.0;
+            if (active) {
+                double kad[CARRY ? 1 : S::NSA][CARRY ? 1 : S::NSD];
+                double kbd[S::NSB][S::NSD];
+                if constexpr (!CARRY) {
 #pragma unroll
-                        for (int e = 0; e < S::NSAB; ++e) s += V[e] * dm(a0 + e / S::NSB, b0 + e % S::NSB);
-                        atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, fj * s);
-                        const double dcd = dm(c0 + sc, d0 + sd);
+                    for (int a = 0; a < S::NSA; ++a)
 #pragma unroll
-                        for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
+                        for (int d = 0; d < S::NSD; ++d) kad[a][d] = 0.0;
+                }
+#pragma unroll
+                for (int bq = 0; bq < S::NSB; ++bq)
+#pragma unroll
+                    for (int d = 0; d < S::NSD; ++d) kbd[bq][d] = 0.0;
+                sfor<S::NSC>([&](auto SC) {
+                    constexpr int sc = TLNO_CI(SC);
+                    double kac[CARRY ? 1 : S::NSA], kbc[S::NSB];
+                    if constexpr (!CARRY) {
+#pragma unroll
+                        for (int a = 0; a < S::NSA; ++a) kac[a] = 0.0;
                     }
-                    if (cl.want_k) {
 #pragma unroll
-                        for (int sa = 0; sa < S::NSA; ++sa) {
-                            const double dad = dm(a0 + sa, d0 + sd), dac = dm(a0 + sa, c0 + sc);
+                    for (int bq = 0; bq < S::NSB; ++bq) kbc[bq] = 0.0;
+                    bool own_sc = false;
+                    sfor<S::NSD>([&](auto SD) {
+                        constexpr int sd = TLNO_CI(SD);
+                        constexpr int t = sc * S::NSD + sd;
+                        const bool own = S::BY_SC ? (sc % S::TPQ == g) : (t % S::TPQ == g);
+                        if (!own) return;
+                        own_sc = true;
+                        double V[S::NSAB];
+                        sfor<S::NSA>([&](auto SA) {
+                            sfor<S::NSB>([&](auto SB) {
+                                constexpr int sa = TLNO_CI(SA), sb = TLNO_CI(SB);
+                                V[sa * S::NSB + sb] = pair_transfer<LA, LB, sa, sb, S::OFA>(
+                                    q.AB, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
+                            });
+                        });
+                        if (cl.want_j) {
+                            double s = 0.0;
 #pragma unroll
-                            for (int sb = 0; sb < S::NSB; ++sb) {
-                                const double v = V[sa * S::NSB + sb];
-                                kac[sa] += v * dm(b0 + sb, d0 + sd);
-                                kad[sa][sd] += v * dm(b0 + sb, c0 + sc);
-                                kbc[sb] += v * dad;
-                                kbd[sb][sd] += v * dac;
+                            for (int e = 0; e < S::NSAB; ++e) s += V[e] * dm(a0 + e / S::NSB, b0 + e % S::NSB);
+                            if constexpr (CARRY)
+                                jcd[t] += fj * s;
+                            else
+                                atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, fj * s);
+                            const double dcd = dm(c0 + sc, d0 + sd);
+#pragma unroll
+                            for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
+                        }
+                        if (cl.want_k) {
+#pragma unroll
+                            for (int sa = 0; sa < S::NSA; ++sa) {
+                                const double dad = dm(a0 + sa, d0 + sd), dac = dm(a0 + sa, c0 + sc);
+                                double sac = 0.0, sad = 0.0;
+#pragma unroll
+                                for (int sb = 0; sb < S::NSB; ++sb) {
+                                    const double v = V[sa * S::NSB + sb];
+                                    sac += v * dm(b0 + sb, d0 + sd);
+                                    sad += v * dm(b0 + sb, c0 + sc);
+                                    kbc[sb] += v * dad;
+                                    kbd[sb][sd] += v * dac;
+                                }
+                                if constexpr (CARRY) {
+                                    kacc[sa][sc] += fk * sac;
+                                    kadc[sa][sd] += fk * sad;
+                                } else {
+                                    kac[sa] += sac;
+                                    kad[sa][sd] += sad;
+                                }
                             }
                         }
+                    });
+                    if (cl.want_k && own_sc) {
+                        if constexpr (!CARRY) {
+#pragma unroll
+                            for (int sa = 0; sa < S::NSA; ++sa)
+                                atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, fk * kac[sa]);
+                        }
+#pragma unroll
+                        for (int sb = 0; sb < S::NSB; ++sb)
+                            atomicAdd(Km + (long long)(b0 + sb) * M + c0 + sc, fk * kbc[sb]);
                     }
                 });
-                if (cl.want_k && own_sc) {
+                if (cl.want_k) {
+                    sfor<S::NSD>([&](auto SD) {
+                        constexpr int sd = TLNO_CI(SD);
+                        bool own_d = false;
 #pragma unroll
-                    for (int sa = 0; sa < S::NSA; ++sa) atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, fk * kac[sa]);
+                        for (int sc = 0; sc < S::NSC; ++sc)
+                            own_d = own_d || (S::BY_SC ? (sc % S::TPQ == g) : ((sc * S::NSD + sd) % S::TPQ == g));
+                        if (!own_d) return;
+                        if constexpr (!CARRY) {
 #pragma unroll
-                    for (int sb = 0; sb < S::NSB; ++sb) atomicAdd(Km + (long long)(b0 + sb) * M + c0 + sc, fk * kbc[sb]);
+                            for (int sa = 0; sa < S::NSA; ++sa)
+                                atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, fk * kad[sa][sd]);
+                        }
+#pragma unroll
+                        for (int sb = 0; sb < S::NSB; ++sb)
+                            atomicAdd(Km + (long long)(b0 + sb) * M + d0 + sd, fk * kbd[sb][sd]);
+                    });
                 }
-            });
-            if (cl.want_k) {
-                sfor<S::NSD>([&](auto SD) {
-                    constexpr int sd = TLNO_CI(SD);
-                    bool own_d = false;
+            }
+            if (cl.want_j) {
+                // J[ab]: every lane of the warp shares the bra pair.
 #pragma unroll
-                    for (int sc = 0; sc < S::NSC; ++sc)
-                        own_d = own_d || (S::BY_SC ? (sc % S::TPQ == g) : ((sc * S::NSD + sd) % S::TPQ == g));
-                    if (!own_d) return;
+                for (int e = 0; e < S::NSAB; ++e) {
+                    double s = fj * jab[e];
 #pragma unroll
-                    for (int sa = 0; sa < S::NSA; ++sa) atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, fk * kad[sa][sd]);
+                    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                    if (lane == 0 && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
+                }
+            }
+            if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
+        }
+
+        if constexpr (CARRY) {
+            // Flush the block's carried ket-side sums (a0 is common to the block).
+            if (touched) {
+                if (cl.want_j) {
 #pragma unroll
-                    for (int sb = 0; sb < S::NSB; ++sb) atomicAdd(Km + (long long)(b0 + sb) * M + d0 + sd, fk * kbd[sb][sd]);
-                });
+                    for (int t = 0; t < S::NSCD; ++t)
+                        atomicAdd(Jm + (long long)(c0 + t / S::NSD) * M + d0 + t % S::NSD, jcd[t]);
+                }
+                if (cl.want_k) {
+#pragma unroll
+                    for (int sa = 0; sa < S::NSA; ++sa) {
+#pragma unroll
+                        for (int sc = 0; sc < S::NSC; ++sc) atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, kacc[sa][sc]);
+#pragma unroll
+                        for (int sd = 0; sd < S::NSD; ++sd) atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, kadc[sa][sd]);
+                    }
+                }
             }
         }
-        if (cl.want_j) {
-            // J[ab]: every lane of the warp shares the bra pair.
-#pragma unroll
-            for (int e = 0; e < S::NSAB; ++e) {
-                double s = fj * jab[e];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0 && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
-            }
-        }
-        if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
     }
     }
 }
@@ -505,7 +587,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_warps() { return FastShape<LA, LB, LC, LD>::WARPS; }
 template <int LA, int LB, int LC, int LD>
-constexpr int fast_bras() { return 1; }
+constexpr int fast_bras() { return FastShape<LA, LB, LC, LD>::GB; }
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_smem_bytes() { return FastShape<LA, LB, LC, LD>::SMEM_DOUBLES * 8; }
 

@@ -344,8 +344,8 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
         const int b = find_block(cl.tile_prefix, cl.n_blocks, tile);
         const int kb = tile - __ldg(cl.tile_prefix + b);
         const BlockDesc bd = cl.blocks[b];
-        const int i = bd.ilocal0;  // bb == 1
-        const int bra = bd.bra0;
+        const int bra = __ldg(cl.bra_list + bd.bra0);  // one bra per block
+        const int i = bra - bd.xbeg;
         const double qi = pv.pair_Q[bra];
         for (int jj = warp; jj < cl.bk; jj += warps) {
             const int j = kb * cl.bk + jj;

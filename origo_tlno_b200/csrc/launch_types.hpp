@@ -27,15 +27,17 @@ struct PlanView {
     const int* mol_M;
 };
 
-// One block of a quartet-class schedule: up to `nbra` consecutive bra pairs
-// against one segment of the ket class list of the same molecule (the kets
-// of a segment share their primitive count and are sorted by Schwarz bound).
+// One block of a quartet-class schedule: `nbra` bra pairs (entries bra0 ..
+// bra0+nbra-1 of the launch's bra list; for the compile-time kernels they
+// share their first shell) against one segment of the ket class list of the
+// same molecule (the kets of a segment share their primitive count).
 struct BlockDesc {
-    int bra0;      // first bra pair (global sorted index)
+    int bra0;      // first entry in ClassLaunch::bra_list
     int nbra;      // bras in this block
     int ket0;      // first pair of the ket segment (global sorted index)
     int nket;      // length of the segment
-    int ilocal0;   // position of bra0 inside its own class list (triangle test)
+    int xbeg;      // first pair of the bra class list of this molecule
+                   // (triangle test on the diagonal class: i = bra - xbeg)
     int koff;      // position of the segment inside the ket class list
 };
 
@@ -45,6 +47,7 @@ struct ClassLaunch {
     int same;                     // bra class == ket class (triangle j <= i)
     int bb, bk;                   // tile shape: bra pairs x ket pairs
     const BlockDesc* blocks;
+    const int* bra_list;          // bra pair (global sorted index) per block entry
     const int* tile_prefix;       // per block: first tile index (n_blocks + 1)
     int n_blocks;
     int tile_begin, tile_end;     // tile range of this launch

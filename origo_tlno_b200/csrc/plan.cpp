@@ -473,29 +473,48 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                             cs.prim_quartets += np * np * n;
                         }
                 }
-                for (int i0 = 0; i0 < nX; i0 += cs.bb) {
-                    const int nbra = std::min(cs.bb, nX - i0);
+                // Bra order: the class list order, or (bra groups) grouped by
+                // first shell A inside each primitive-count group, list order
+                // kept inside a group; a block holds up to cs.bb bras of one A.
+                std::vector<int> order(nX);
+                for (int i = 0; i < nX; ++i) order[i] = i;
+                if (cs.bb > 1)
+                    std::stable_sort(order.begin(), order.end(), [&](int u, int v) {
+                        const int nu = plan.pair_nprim[bx0 + u], nv = plan.pair_nprim[bx0 + v];
+                        if (nu != nv) return nu < nv;
+                        return plan.pair_A[bx0 + u] < plan.pair_A[bx0 + v];
+                    });
+                for (int i0 = 0; i0 < nX;) {
+                    int nbra = 1;
+                    if (cs.bb > 1)
+                        while (nbra < cs.bb && i0 + nbra < nX &&
+                               plan.pair_A[bx0 + order[i0 + nbra]] == plan.pair_A[bx0 + order[i0]])
+                            ++nbra;
+                    const int brabeg = static_cast<int>(cs.bra_list.size());
+                    bool used = false;
                     for (std::size_t sg = 0; sg + 1 < seg.size(); ++sg) {
                         const int s0 = seg[sg], s1 = seg[sg + 1];
-                        const long long npk = plan.pair_nprim[by0 + s0];
                         int ext = 0;
-                        // exact statistics per bra
                         for (int w = 0; w < nbra; ++w) {
-                            const int i = i0 + w;
+                            const int i = order[i0 + w];
                             ext = std::max(ext, seg_extent(plan.pair_Q[bx0 + i], s0, s1, i));
                         }
                         const int nt = (ext + cs.bk - 1) / cs.bk;
                         if (nt <= 0) continue;
+                        used = true;
                         dev::BlockDesc bd{};
-                        bd.bra0 = bx0 + i0;
+                        bd.bra0 = brabeg;
                         bd.nbra = nbra;
                         bd.ket0 = by0 + s0;
                         bd.nket = s1 - s0;
-                        bd.ilocal0 = i0;
+                        bd.xbeg = bx0;
                         bd.koff = s0;
                         cs.blocks.push_back(bd);
                         cs.prefix.push_back(cs.prefix.back() + nt);
                     }
+                    if (used)
+                        for (int w = 0; w < nbra; ++w) cs.bra_list.push_back(bx0 + order[i0 + w]);
+                    i0 += nbra;
                 }
             }
             cs.n_tiles = cs.prefix.back();
@@ -503,6 +522,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
             cs.flops = fprim * cs.prim_quartets + fcon * cs.quartets;
             upload_vec(cs.d_blocks, cs.blocks, s);
             upload_vec(cs.d_prefix, cs.prefix, s);
+            upload_vec(cs.d_bra_list, cs.bra_list, s);
             plan.total_quartets += cs.quartets;
             plan.total_prim_quartets += cs.prim_quartets;
             plan.total_flops += cs.flops;

@@ -26,7 +26,8 @@ struct ComboSchedule {
     int bb = 1, bk = 16;
     std::vector<dev::BlockDesc> blocks;
     std::vector<int> prefix;
-    DeviceBuffer d_blocks, d_prefix;
+    std::vector<int> bra_list;
+    DeviceBuffer d_blocks, d_prefix, d_bra_list;
     int n_tiles = 0;
     long long quartets = 0;       // surviving contracted quartets
     long long prim_quartets = 0;  // surviving primitive quartets
