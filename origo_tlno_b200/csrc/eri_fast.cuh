@@ -79,7 +79,7 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
 constexpr int kMaxAccPerSlice = 64;
 constexpr int kTileChunk = 4;  // tiles per dynamic-schedule fetch
 constexpr int kBraGroup = 8;   // bras per block of the light classes
-constexpr int kMaxCarried = 16;
+constexpr int kMaxCarried = 24;
 
 __host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
     int t = 1;
@@ -207,30 +207,53 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
     if (active) {
         const int npb = __ldg(pv.pair_nprim + bra), npk = __ldg(pv.pair_nprim + ket);
-        // 48-byte records {p, Px, Py, Pz, w, 1/p} read as three 16-byte vectors.
-        const double2* pb = reinterpret_cast<const double2*>(pv.prim + __ldg(pv.pair_prim_off + bra));
-        const double2* pk = reinterpret_cast<const double2*>(pv.prim + __ldg(pv.pair_prim_off + ket));
+        const int ob = __ldg(pv.pair_prim_off + bra), ok = __ldg(pv.pair_prim_off + ket);
+        // FP64: 48-byte records {p, Px, Py, Pz, w, 1/p} read as three 16-byte
+        // vectors.  FP32: 24-byte records {p, P-A, w, 1/p} relative to the
+        // pair's first centre, PQ = (P-A) - (Q-C) + (A-C).
+        const double2* pb = reinterpret_cast<const double2*>(pv.prim + ob);
+        const double2* pk = reinterpret_cast<const double2*>(pv.prim + ok);
+        const float2* pb32 = reinterpret_cast<const float2*>(pv.prim32 + ob);
+        const float2* pk32 = reinterpret_cast<const float2*>(pv.prim32 + ok);
+        constexpr bool F32 = std::is_same<R, float>::value;
+        const R ACx = R(q.A[0] - q.C[0]), ACy = R(q.A[1] - q.C[1]), ACz = R(q.A[2] - q.C[2]);
         for (int ib = 0; ib < npb; ++ib) {
-            const double2 b0v = __ldg(pb + 3 * ib), b1v = __ldg(pb + 3 * ib + 1), b2v = __ldg(pb + 3 * ib + 2);
-            const double bp_p = b0v.x, bp_x = b0v.y, bp_y = b1v.x, bp_z = b1v.y, bp_w = b2v.x, bp_ip = b2v.y;
-            const R p = R(bp_p);
-            const R PAx = R(bp_x - q.A[0]), PAy = R(bp_y - q.A[1]), PAz = R(bp_z - q.A[2]);
+            R p, PAx, PAy, PAz, bw, bip;
+            double bp_x = 0.0, bp_y = 0.0, bp_z = 0.0;
+            if constexpr (F32) {
+                const float2 u0 = __ldg(pb32 + 3 * ib), u1 = __ldg(pb32 + 3 * ib + 1), u2 = __ldg(pb32 + 3 * ib + 2);
+                p = u0.x; PAx = u0.y; PAy = u1.x; PAz = u1.y; bw = u2.x; bip = u2.y;
+            } else {
+                const double2 b0v = __ldg(pb + 3 * ib), b1v = __ldg(pb + 3 * ib + 1), b2v = __ldg(pb + 3 * ib + 2);
+                bp_x = b0v.y; bp_y = b1v.x; bp_z = b1v.y;
+                p = R(b0v.x);
+                PAx = R(bp_x - q.A[0]); PAy = R(bp_y - q.A[1]); PAz = R(bp_z - q.A[2]);
+                bw = R(b2v.x); bip = R(b2v.y);
+            }
             for (int ik = 0; ik < npk; ++ik) {
-                const double2 k0v = __ldg(pk + 3 * ik), k1v = __ldg(pk + 3 * ik + 1), k2v = __ldg(pk + 3 * ik + 2);
-                const double kp_p = k0v.x, kp_x = k0v.y, kp_y = k1v.x, kp_z = k1v.y, kp_w = k2v.x, kp_ip = k2v.y;
-                const R qe = R(kp_p);
+                R qe, QCx, QCy, QCz, kw, kip, PQx, PQy, PQz;
+                if constexpr (F32) {
+                    const float2 u0 = __ldg(pk32 + 3 * ik), u1 = __ldg(pk32 + 3 * ik + 1), u2 = __ldg(pk32 + 3 * ik + 2);
+                    qe = u0.x; QCx = u0.y; QCy = u1.x; QCz = u1.y; kw = u2.x; kip = u2.y;
+                    PQx = PAx - QCx + ACx; PQy = PAy - QCy + ACy; PQz = PAz - QCz + ACz;
+                } else {
+                    const double2 k0v = __ldg(pk + 3 * ik), k1v = __ldg(pk + 3 * ik + 1), k2v = __ldg(pk + 3 * ik + 2);
+                    const double kp_x = k0v.y, kp_y = k1v.x, kp_z = k1v.y;
+                    qe = R(k0v.x);
+                    QCx = R(kp_x - q.C[0]); QCy = R(kp_y - q.C[1]); QCz = R(kp_z - q.C[2]);
+                    kw = R(k2v.x); kip = R(k2v.y);
+                    PQx = R(bp_x - kp_x); PQy = R(bp_y - kp_y); PQz = R(bp_z - kp_z);
+                }
                 const R pqs = p + qe;
                 // one reciprocal square root gives both 1/sqrt(p+q) and 1/(p+q)
                 const R rs = rsqrt(pqs);
                 const R inv = rs * rs;
-                const R PQx = R(bp_x - kp_x), PQy = R(bp_y - kp_y), PQz = R(bp_z - kp_z);
                 const R Targ = p * qe * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
                 R rt[S::N], wt[S::N];
                 rys_roots_all<R, S::N>(Targ, rt, wt);
-                const R pref = R(34.98683665524972497) * R(bp_w) * R(kp_w) * rs;
+                const R pref = R(34.98683665524972497) * bw * kw * rs;
                 const R qo = qe * inv, po = p * inv;
-                const R hbp = R(0.5) * R(bp_ip), hkp = R(0.5) * R(kp_ip);
-                const R QCx = R(kp_x - q.C[0]), QCy = R(kp_y - q.C[1]), QCz = R(kp_z - q.C[2]);
+                const R hbp = R(0.5) * bip, hkp = R(0.5) * kip;
 #pragma unroll
                 for (int r = 0; r < S::N; ++r) {
                     const R t2 = rt[r];

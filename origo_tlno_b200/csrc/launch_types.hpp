@@ -9,6 +9,12 @@ struct DPrimPair {
     double p, Px, Py, Pz, w, invp;
 };
 
+// FP32 copy for the mixed-precision kernels: P relative to the pair's first
+// centre A, so that FP32 never subtracts two absolute coordinates.
+struct FPrimPair {
+    float p, PAx, PAy, PAz, w, invp;
+};
+
 // Device view of one plan (or of a batch of plans: every pair carries the
 // AO offset of its molecule, so one launch can serve many molecules).
 struct PlanView {
@@ -22,6 +28,7 @@ struct PlanView {
     const double* pair_Q;         // Schwarz bound
     const int* pair_mol;          // molecule of the pair (batch), may be null
     const DPrimPair* prim;
+    const FPrimPair* prim32;      // same records in FP32 (P relative to A), may be null
     // Per-molecule matrix bases (batch): density/J/K at base + M*M offsets.
     const long long* mol_mat_off; // element offset of the molecule's M x M block
     const int* mol_M;

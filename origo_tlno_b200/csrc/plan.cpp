@@ -284,6 +284,7 @@ dev::PlanView Plan2e::view() const {
     pv.pair_Q = d_pair_Q.as<double>();
     pv.pair_mol = n_mol > 1 ? d_pair_mol.as<int>() : nullptr;
     pv.prim = d_prim.as<dev::DPrimPair>();
+    pv.prim32 = d_prim32.as<dev::FPrimPair>();
     pv.mol_mat_off = n_mol > 1 ? d_mol_mat_off.as<long long>() : nullptr;
     pv.mol_M = n_mol > 1 ? d_mol_M.as<int>() : nullptr;
     return pv;
@@ -336,6 +337,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
     }
     plan.kept_pairs = static_cast<long long>(plan.pair_A.size());
     std::vector<dev::DPrimPair> prim(static_cast<std::size_t>(prim_total));
+    std::vector<dev::FPrimPair> prim32(static_cast<std::size_t>(prim_total));
     {
         const long long np = static_cast<long long>(plan.pair_A.size());
         parallel_for(np, [&](long long b0, long long e0) {
@@ -346,6 +348,13 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                 tmp.clear();
                 primitive_pairs(*bases[m], plan.pair_A[k] - so, plan.pair_B[k] - so, tmp);
                 std::copy(tmp.begin(), tmp.end(), prim.begin() + plan.pair_prim_off[k]);
+                const auto& ca = bases[m]->shells[plan.pair_A[k] - so].center;
+                for (std::size_t t = 0; t < tmp.size(); ++t) {
+                    const dev::DPrimPair& d = tmp[t];
+                    prim32[plan.pair_prim_off[k] + t] = {static_cast<float>(d.p), static_cast<float>(d.Px - ca[0]),
+                                                         static_cast<float>(d.Py - ca[1]), static_cast<float>(d.Pz - ca[2]),
+                                                         static_cast<float>(d.w), static_cast<float>(d.invp)};
+                }
             }
         });
     }
@@ -359,6 +368,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
     upload_vec(plan.d_pair_Q, plan.pair_Q, s);
     upload_vec(plan.d_pair_mol, plan.pair_mol, s);
     upload_vec(plan.d_prim, prim, s);
+    upload_vec(plan.d_prim32, prim32, s);
     upload_vec(plan.d_mol_mat_off, plan.mol_mat_off, s);
     upload_vec(plan.d_mol_M, plan.mol_M, s);
 

@@ -59,7 +59,7 @@ public:
     DeviceBuffer d_counters;  // dynamic-schedule counters, 2 per combo (FP64 and FP32 pass)
     DeviceBuffer d_shell_xyz, d_shell_L, d_shell_sph;
     DeviceBuffer d_pair_A, d_pair_B, d_pair_prim_off, d_pair_nprim, d_pair_Q, d_pair_mol;
-    DeviceBuffer d_prim, d_mol_mat_off, d_mol_M;
+    DeviceBuffer d_prim, d_prim32, d_mol_mat_off, d_mol_M;
     long long total_quartets = 0, total_prim_quartets = 0;
     double total_flops = 0.0;
     long long total_pairs = 0, kept_pairs = 0;
