@@ -272,6 +272,12 @@ def run_native(args):
     # FP64 sequence first (also the accuracy reference for the last density)
     ms64 = timed_sequence(False)
     J64, K64 = J.clone(), K.clone()
+    # split threshold of the mixed path: autotuned on the last density
+    # against its FP64 build, 10x inside the accuracy targets
+    tune = None
+    if not args.no_autotune:
+        from origo_tlno_b200.autotune import tune_mixed_threshold
+        tune = tune_mixed_threshold(ctx, Ds[-1], tol_energy=1e-7, tol_jk=1e-8, reference=(J64, K64))
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -346,7 +352,8 @@ def run_native(args):
                    "flops_per_build_model": prof["flops"], "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (D, J, K are M*M*8 bytes each)" if M * M * 8 > 126e6 else
                          "inputs smaller than L2",
-                   "mixed_threshold": args.mixed_threshold, "schwarz": tau},
+                   "mixed_threshold": tune["threshold"] if tune else args.mixed_threshold, "schwarz": tau},
+        "mixed_autotune": tune,
         "jk_builds_per_s": ws * steps / tmx,
         "fp64": {"value": value64, "unit": UNIT, "jk_builds_per_s": ws * steps / t64,
                  "ms_per_step": 1e3 * t64 / steps},
@@ -382,6 +389,8 @@ def main():
     ap.add_argument("--config", default="cfg4")
     ap.add_argument("--mixed-threshold", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep --mixed-threshold instead of autotuning the split threshold")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

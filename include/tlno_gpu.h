@@ -131,6 +131,13 @@ int tlno_gpu_onee(tlno_gpu_context* ctx, double* S, double* T, double* V, int sc
 int tlno_gpu_set_onee_thresholds(tlno_gpu_context* ctx, double group_pair_decay_eps,
                                  double nuclear_screen_eps);
 
+/* Split threshold of the mixed-precision J/K path (quartets with
+ * Q_ab Q_cd max|D| below it run in FP32), as ScreeningOptions.mixed_threshold
+ * without re-planning; used by the split-threshold autotuner.  No reference
+ * counterpart (the reference has no mixed-precision path).  A captured J/K
+ * graph keeps the value of its capture: capture again after a change. */
+int tlno_gpu_set_mixed_threshold(tlno_gpu_context* ctx, double mixed_threshold);
+
 /* Contracted spherical ERI blocks (A B | C D) for n quartets of shell
  * indices (4 per quartet); block q is written at out + offsets[q] with layout
  * [(2La+1)(2Lb+1)] x [(2Lc+1)(2Ld+1)] row-major.  Host buffers.  The

@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
         "tlno_gpu_jk": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
         "tlno_gpu_onee": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
         "tlno_gpu_set_onee_thresholds": (C.c_int, [_vp, C.c_double, C.c_double]),
+        "tlno_gpu_set_mixed_threshold": (C.c_int, [_vp, C.c_double]),
         "tlno_gpu_eri_blocks": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
         "tlno_gpu_eri_blocks_noalloc": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
         "tlno_gpu_schwarz": (C.c_int, [_vp, _vp]),
@@ -135,6 +136,7 @@ EXPORTED = [
     "tlno_gpu_last_error", "tlno_gpu_version", "tlno_gpu_device_count", "tlno_gpu_create",
     "tlno_gpu_create_from_components", "tlno_gpu_destroy", "tlno_gpu_n_sph", "tlno_gpu_n_shells",
     "tlno_gpu_plan", "tlno_gpu_plan_profile", "tlno_gpu_jk", "tlno_gpu_onee", "tlno_gpu_set_onee_thresholds",
+    "tlno_gpu_set_mixed_threshold",
     "tlno_gpu_eri_blocks", "tlno_gpu_eri_blocks_noalloc", "tlno_gpu_schwarz", "tlno_gpu_boys", "tlno_gpu_rys", "tlno_gpu_fma_peak",
     "tlno_gpu_jk_graph_capture",
     "tlno_gpu_jk_graph_launch", "tlno_gpu_synchronize", "tlno_gpu_stream", "tlno_gpu_batch_create",

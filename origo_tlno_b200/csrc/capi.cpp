@@ -356,6 +356,15 @@ int tlno_gpu_set_onee_thresholds(tlno_gpu_context* ctx, double group_pair_decay_
     });
 }
 
+int tlno_gpu_set_mixed_threshold(tlno_gpu_context* ctx, double mixed_threshold) {
+    return guarded([&] {
+        if (!ctx) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null context");
+        if (!finite_bits(mixed_threshold) || mixed_threshold < 0.0)
+            throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: mixed_threshold must be finite and >= 0.");
+        ctx->screening.mixed_threshold = mixed_threshold;
+    });
+}
+
 int tlno_gpu_onee(tlno_gpu_context* ctx, double* S, double* T, double* V, int screening, int flags) {
     return guarded([&] {
         if (!ctx || !S || !T || !V) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");

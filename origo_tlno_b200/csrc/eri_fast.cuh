@@ -391,9 +391,31 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         const bool lane_ok = j < bd.nket;
         const int ket = bd.ket0 + (lane_ok ? j : 0);
 
+        // Quick test on the Schwarz products alone: a tile without any quartet
+        // for this launch (bound, triangle, precision pass) is left before
+        // the ket geometry is loaded.
+        const double qket = __ldg(pv.pair_Q + ket);
+        {
+            bool act = false;
+            for (int ib = 0; ib < S::GB && ib < bd.nbra; ++ib) {
+                const int bra = __ldg(cl.bra_list + bd.bra0 + ib);
+                if (!lane_ok || (cl.same && bd.koff + j > bra - bd.xbeg)) continue;
+                const double qq = __ldg(pv.pair_Q + bra) * qket;
+                bool a = qq >= cl.tau;
+                if (cl.prec_mode == 1) a = a && qq >= thr;
+                if (cl.prec_mode == 2) a = a && !(qq >= thr);
+                act = act || a;
+            }
+            bool any_tile;
+            if constexpr (S::TPQ > 1)
+                any_tile = group_any(act, bar_id, bar_n);
+            else
+                any_tile = __any_sync(0xffffffffu, act);
+            if (!any_tile) continue;
+        }
+
         // ket side, once per tile
         const int C = __ldg(pv.pair_A + ket), D = __ldg(pv.pair_B + ket);
-        const double qket = __ldg(pv.pair_Q + ket);
         QuartetGeom q;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {

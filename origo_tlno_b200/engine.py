@@ -186,6 +186,13 @@ class Context:
         N.check(N.lib().tlno_gpu_onee(self.h, N.ptr(S), N.ptr(T), N.ptr(V), 1 if screening else 0, 0))
         return S, T, V
 
+    def set_mixed_threshold(self, threshold: float):
+        """Split threshold of the mixed-precision path without re-planning
+        (recapture any J/K graph afterwards)."""
+        N.check(N.lib().tlno_gpu_set_mixed_threshold(self.h, threshold))
+        if getattr(self, "options", None) is not None:
+            self.options.mixed_threshold = threshold
+
     def set_onee_thresholds(self, decay_eps: float, nuclear_eps: float):
         N.check(N.lib().tlno_gpu_set_onee_thresholds(self.h, decay_eps, nuclear_eps))
 

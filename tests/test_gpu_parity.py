@@ -116,6 +116,28 @@ def test_jk_cfg1_mixed(ctx1):
     assert abs(e - e_ref) < 1e-6
 
 
+def test_mixed_threshold_autotune_cfg1():
+    # the autotuner keeps the largest split threshold whose mixed build stays
+    # within its tolerances of the FP64 build, and sets it on the context
+    import torch
+    from origo_tlno_b200.autotune import tune_mixed_threshold
+    mol = M.cfg1()
+    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=1e-12))
+    D = torch.tensor(M.density_for("cfg1", mol), device="cuda")
+    res = tune_mixed_threshold(ctx, D, candidates=(1e-3, 1e-6, 1e-9), tol_energy=1e-7, tol_jk=1e-8)
+    assert res["trials"] and res["trials"][-1]["ok"]
+    assert res["threshold"] == res["trials"][-1]["threshold"]
+    for t in res["trials"][:-1]:
+        assert not t["ok"]
+    out = ctx.jk(D.cpu().numpy(), mixed=True)
+    ref = ctx.jk(D.cpu().numpy(), mixed=False)
+    assert np.max(np.abs(out["J"] - ref["J"])) <= 1e-8
+    assert np.max(np.abs(out["K"] - ref["K"])) <= 1e-8
+    with pytest.raises(E.TlnoError, match="mixed_threshold"):
+        ctx.set_mixed_threshold(float("nan"))
+    ctx.close()
+
+
 def test_onee_cfg0(ctx0):
     g = load_golden("cfg0.npz")
     S, T, V = ctx0.onee(screening=True)
