@@ -158,6 +158,82 @@ namespace tlno_gpu {
 #define TLNO_FAST_IF_20(x)
 #endif
 
+#if TLNO_FAST_ID == 21
+#define TLNO_FAST_IF_21(x) x
+#else
+#define TLNO_FAST_IF_21(x)
+#endif
+#if TLNO_FAST_ID == 22
+#define TLNO_FAST_IF_22(x) x
+#else
+#define TLNO_FAST_IF_22(x)
+#endif
+#if TLNO_FAST_ID == 23
+#define TLNO_FAST_IF_23(x) x
+#else
+#define TLNO_FAST_IF_23(x)
+#endif
+#if TLNO_FAST_ID == 24
+#define TLNO_FAST_IF_24(x) x
+#else
+#define TLNO_FAST_IF_24(x)
+#endif
+#if TLNO_FAST_ID == 25
+#define TLNO_FAST_IF_25(x) x
+#else
+#define TLNO_FAST_IF_25(x)
+#endif
+#if TLNO_FAST_ID == 26
+#define TLNO_FAST_IF_26(x) x
+#else
+#define TLNO_FAST_IF_26(x)
+#endif
+#if TLNO_FAST_ID == 27
+#define TLNO_FAST_IF_27(x) x
+#else
+#define TLNO_FAST_IF_27(x)
+#endif
+#if TLNO_FAST_ID == 28
+#define TLNO_FAST_IF_28(x) x
+#else
+#define TLNO_FAST_IF_28(x)
+#endif
+#if TLNO_FAST_ID == 29
+#define TLNO_FAST_IF_29(x) x
+#else
+#define TLNO_FAST_IF_29(x)
+#endif
+#if TLNO_FAST_ID == 30
+#define TLNO_FAST_IF_30(x) x
+#else
+#define TLNO_FAST_IF_30(x)
+#endif
+#if TLNO_FAST_ID == 31
+#define TLNO_FAST_IF_31(x) x
+#else
+#define TLNO_FAST_IF_31(x)
+#endif
+#if TLNO_FAST_ID == 32
+#define TLNO_FAST_IF_32(x) x
+#else
+#define TLNO_FAST_IF_32(x)
+#endif
+#if TLNO_FAST_ID == 33
+#define TLNO_FAST_IF_33(x) x
+#else
+#define TLNO_FAST_IF_33(x)
+#endif
+#if TLNO_FAST_ID == 34
+#define TLNO_FAST_IF_34(x) x
+#else
+#define TLNO_FAST_IF_34(x)
+#endif
+#if TLNO_FAST_ID == 35
+#define TLNO_FAST_IF_35(x) x
+#else
+#define TLNO_FAST_IF_35(x)
+#endif
+
 TLNO_FAST_CLASSES(TLNO_FAST_SELECT)
 
 }  // namespace tlno_gpu

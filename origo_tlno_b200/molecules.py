@@ -237,6 +237,26 @@ def cfg4() -> Molecule:
     return water_cluster(400, 5)
 
 
+def fragment(mol: Molecule, atoms: Sequence[int], name: str = "") -> Molecule:
+    """The sub-molecule of the listed atoms with their shells (same
+    exponents and coefficients), atoms renumbered in the given order."""
+    atoms = [int(a) for a in atoms]
+    remap = {a: k for k, a in enumerate(atoms)}
+    out = Molecule(name or f"{mol.name}_frag", mol.charges[atoms].copy(), mol.coords[atoms].copy())
+    for a in atoms:
+        for sh in mol.shells:
+            if sh.atom == a:
+                out.shells.append(ShellSpec(sh.center, sh.L, sh.exponents.copy(), sh.coefficients.copy(),
+                                            atom=remap[a]))
+    return out
+
+
+def cfg2_fragment() -> Molecule:
+    """Two heavy atoms and one hydrogen of cfg2 (shells up to f, M = 74):
+    the f-shell parity case."""
+    return fragment(cfg2(), [0, 1, 40], "cfg2_fragment")
+
+
 def random_density(n_bf: int, n_occ: int, seed: int) -> np.ndarray:
     """D = C C^T with C (n_bf x n_occ) ~ N(0,1)/sqrt(n_bf)."""
     rng = np.random.default_rng(seed)

@@ -10,6 +10,9 @@ Fixtures (float64, npz):
                shell-quartet ERI block, Schwarz bounds per shell pair.
   cfg1.npz  -- cfg1 (24 atoms, M = 246): S, T, V, J, K at Schwarz 1e-12,
                Schwarz bounds, and 200 sampled ERI blocks.
+  cfg2f.npz -- two heavy atoms and one H of cfg2 (shells up to f, M = 74):
+               S, T, V, J, K at Schwarz 1e-12 for a random density (seed
+               21), and 300 sampled ERI blocks, every one holding an f shell.
   boys.npz  -- reference Boys values F_n(x) (core/math/general_math.cpp
                boys_single) on edge and interior arguments.
   rys.npz   -- reference Rys roots/weights (production table path) for
@@ -49,6 +52,22 @@ def blocks(rb, quads):
         vals.append(v)
         offs.append(offs[-1] + v.size)
     return np.concatenate(vals), np.array(offs, dtype=np.int64)
+
+
+def write_cfg2f():
+    mol = M.cfg2_fragment()
+    D = M.random_density(mol.n_sph, 20, seed=21)
+    rb = ref.RefBasis(mol)
+    S, T, V = rb.onee(screening=True)
+    o = rb.jk(D, schwarz=1e-12, want=("J", "K"))
+    Ls = [s.L for s in mol.shells]
+    q = quartet_list(mol)
+    q = q[[max(Ls[a], Ls[b], Ls[c], Ls[d]) == 3 for a, b, c, d in q]]
+    rng = np.random.default_rng(9)
+    q = q[np.sort(rng.choice(len(q), size=300, replace=False))]
+    vals, offs = blocks(rb, q)
+    np.savez_compressed(os.path.join(OUT, "cfg2f.npz"), S=S, T=T, V=V, D=D, J=o["J"], K=o["K"],
+                        quartets=q, eri=vals, eri_off=offs, schwarz=rb.schwarz())
 
 
 def main():
@@ -92,6 +111,7 @@ def main():
             R[n - 1, k, :n] = r
             W[n - 1, k, :n] = w
     np.savez_compressed(os.path.join(OUT, "rys.npz"), T=Ts, roots=R, weights=W)
+    write_cfg2f()
     print("golden fixtures written to", OUT)
 
 

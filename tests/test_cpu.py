@@ -147,6 +147,21 @@ def test_port_cfg1_eri_sample_against_golden(port):
         assert np.max(np.abs(pb.eri_block(a, b, c, d).ravel() - ref)) < 1e-12
 
 
+def test_port_cfg2_fragment_f_shells_against_golden(port):
+    # shells up to f: ERI blocks holding an f shell and the one-electron
+    # matrices of the restatement against the reference's fixture
+    g = load_golden("cfg2f.npz")
+    pb = port.PortBasis(M.cfg2_fragment())
+    for k in range(0, len(g["quartets"]), 5):
+        a, b, c, d = g["quartets"][k]
+        ref = g["eri"][g["eri_off"][k]:g["eri_off"][k + 1]]
+        assert np.max(np.abs(pb.eri_block(a, b, c, d).ravel() - ref)) < 1e-12
+    S, T, V = pb.onee()
+    assert np.max(np.abs(S - g["S"])) < 1e-12
+    assert np.max(np.abs(T - g["T"])) < 1e-12
+    assert np.max(np.abs(V - g["V"])) < 1e-12
+
+
 def test_port_against_compiled_reference_small(port):
     from oracle import ref
     if not ref.available():

@@ -116,6 +116,28 @@ def test_jk_cfg1_mixed(ctx1):
     assert abs(e - e_ref) < 1e-6
 
 
+def test_cfg2_fragment_f_shells():
+    # shells up to f (the warp-per-quartet kernel for every class holding an
+    # f shell): ERI blocks, J/K and S/T/V against the reference's fixture
+    g = load_golden("cfg2f.npz")
+    mol = M.cfg2_fragment()
+    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=1e-12))
+    blocks = ctx.eri_blocks(g["quartets"])
+    err = 0.0
+    for k, blk in enumerate(blocks):
+        ref = g["eri"][g["eri_off"][k]:g["eri_off"][k + 1]].reshape(blk.shape)
+        err = max(err, _maxabs(blk, ref))
+    assert err < 1e-12
+    out = ctx.jk(g["D"])
+    assert _maxabs(out["J"], g["J"]) < 5e-12
+    assert _maxabs(out["K"], g["K"]) < 5e-12
+    S, T, V = ctx.onee()
+    assert _maxabs(S, g["S"]) < 1e-12
+    assert _maxabs(T, g["T"]) < 2e-12
+    assert _maxabs(V, g["V"]) < 1e-12
+    ctx.close()
+
+
 def test_mixed_threshold_autotune_cfg1():
     # the autotuner keeps the largest split threshold whose mixed build stays
     # within its tolerances of the FP64 build, and sets it on the context
