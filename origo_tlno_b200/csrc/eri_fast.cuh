@@ -136,11 +136,11 @@ __device__ __forceinline__ void sfor(F&& f) {
 #define TLNO_CI(x) decltype(x)::value
 
 // HRR transfer coefficient C(B,U) X^(B-U).
-template <int B, int U>
-__device__ __forceinline__ double hrr_coef(double x) {
+template <int B, int U, typename T>
+__device__ __forceinline__ T hrr_coef(T x) {
     constexpr int e = B - U;
-    constexpr double c = double(ce_binom(B, U));
-    if constexpr (e == 0) return 1.0;
+    constexpr T c = T(ce_binom(B, U));
+    if constexpr (e == 0) return T(1);
     else if constexpr (e == 1) return c * x;
     else if constexpr (e == 2) return c * (x * x);
     else if constexpr (e == 3) return c * (x * x * x);
@@ -153,20 +153,20 @@ __device__ __forceinline__ double hrr_coef(double x) {
 // X = centre1 - centre2, then the Cartesian->spherical projection with the
 // angular normalisation folded in.  src(integral_constant<int, f>) returns
 // row f.
-template <int L1, int L2, int S1, int S2, int OF, typename Src>
-__device__ __forceinline__ double pair_transfer(const double* X, Src&& src) {
-    double out = 0.0;
+template <typename T, int L1, int L2, int S1, int S2, int OF, typename Src>
+__device__ __forceinline__ T pair_transfer(const T* X, Src&& src) {
+    T out = T(0);
     sfor<ce_ncart(L1)>([&](auto C1) {
         constexpr int c1 = TLNO_CI(C1);
         if constexpr (c2s_nz(L1, S1, c1)) {
             constexpr int f1 = ce_off(L1) + c1;
-            double row = 0.0;
+            T row = T(0);
             sfor<ce_ncart(L2)>([&](auto C2) {
                 constexpr int c2 = TLNO_CI(C2);
                 if constexpr (c2s_nz(L2, S2, c2)) {
                     constexpr int f2 = ce_off(L2) + c2;
                     constexpr int bx = ce_x(f2), by = ce_y(f2), bz = ce_z(f2);
-                    double h = 0.0;
+                    T h = T(0);
                     sfor<bx + 1>([&](auto UX) {
                         sfor<by + 1>([&](auto UY) {
                             sfor<bz + 1>([&](auto UZ) {
@@ -178,11 +178,11 @@ __device__ __forceinline__ double pair_transfer(const double* X, Src&& src) {
                         });
                     });
                     if constexpr (L2 <= 1) row += h;
-                    else row += c_c2s.dense[L2][S2][c2] * h;
+                    else row += T(c_c2s.dense[L2][S2][c2]) * h;
                 }
             });
             if constexpr (L1 <= 1) out += row;
-            else out += c_c2s.dense[L1][S1][c1] * row;
+            else out += T(c_c2s.dense[L1][S1][c1]) * row;
         }
     });
     return out;
@@ -196,7 +196,7 @@ struct QuartetGeom {
 // Phase 1 + 2 for slice G (rows ia = G, G+TPQ, ...).
 template <typename R, int LA, int LB, int LC, int LD, int G>
 __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
-                                           double* __restrict__ ks) {
+                                           R* __restrict__ ks) {
     using S = FastShape<LA, LB, LC, LD>;
     constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
     R acc[ROWS > 0 ? ROWS : 1][S::NCS];
@@ -299,15 +299,17 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
         }
     }
 
-    // Phase 2: ket transfer + projection of the owned rows.
+    // Phase 2: ket transfer + projection of the owned rows (in R: the FP32
+    // kernels keep the whole quartet in FP32 up to the FP64 atomics).
+    const R CDr[3] = {R(q.CD[0]), R(q.CD[1]), R(q.CD[2])};
     sfor<ROWS>([&](auto RR) {
         constexpr int rr = TLNO_CI(RR);
         constexpr int ia = G + rr * S::TPQ;
         sfor<S::NSC>([&](auto SC) {
             sfor<S::NSD>([&](auto SD) {
                 constexpr int sc = TLNO_CI(SC), sd = TLNO_CI(SD);
-                ks[ia * S::NSCD + sc * S::NSD + sd] = pair_transfer<LC, LD, sc, sd, S::OFC>(
-                    q.CD, [&](auto FU) { return double(acc[rr][TLNO_CI(FU)]); });
+                ks[ia * S::NSCD + sc * S::NSD + sd] = pair_transfer<R, LC, LD, sc, sd, S::OFC>(
+                    CDr, [&](auto FU) { return acc[rr][TLNO_CI(FU)]; });
             });
         });
     });
@@ -315,7 +317,7 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
 template <typename R, int LA, int LB, int LC, int LD, int G = 0>
 __device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, int bra, int ket, bool active,
-                                                    const QuartetGeom& q, double* ks) {
+                                                    const QuartetGeom& q, R* ks) {
     using S = FastShape<LA, LB, LC, LD>;
     if constexpr (G < S::TPQ) {
         if (g == G)
@@ -349,12 +351,12 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     const int grp = warp / S::TPQ, g = warp % S::TPQ;
     // A quartet owned by one thread keeps its (a0|cd) rows in registers; a
     // sliced quartet exchanges them through shared memory.
-    double ks_reg[S::TPQ == 1 ? S::NAS * S::NSCD : 1];
-    double* ks;
+    R ks_reg[S::TPQ == 1 ? S::NAS * S::NSCD : 1];
+    R* ks;
     if constexpr (S::TPQ == 1)
         ks = ks_reg;
     else
-        ks = fast_smem + (grp * 32 + lane) * S::LANE_STRIDE;
+        ks = reinterpret_cast<R*>(fast_smem) + (grp * 32 + lane) * S::LANE_STRIDE;
     const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
     const int bar_id = 1 + grp, bar_n = 32 * S::TPQ;
     __shared__ int s_chunk[S::BBQ];
@@ -434,9 +436,9 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         // Sums carried across the bras of a block (they share the first
         // shell A): J[cd], K[ac], K[ad] of this lane's ket.
         constexpr bool CARRY = S::GB > 1;
-        double jcd[CARRY ? S::NSCD : 1];
-        double kacc[CARRY ? S::NSA : 1][CARRY ? S::NSC : 1];
-        double kadc[CARRY ? S::NSA : 1][CARRY ? S::NSD : 1];
+        R jcd[CARRY ? S::NSCD : 1];
+        R kacc[CARRY ? S::NSA : 1][CARRY ? S::NSC : 1];
+        R kadc[CARRY ? S::NSA : 1][CARRY ? S::NSD : 1];
         if constexpr (CARRY) {
 #pragma unroll
             for (int t = 0; t < S::NSCD; ++t) jcd[t] = 0.0;
@@ -481,18 +483,19 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
             // ---- bra transfer + projection per owned ket column, digestion ----
             a0 = __ldg(pv.shell_sph + A);
             const int b0 = __ldg(pv.shell_sph + B);
-            double f = active ? 1.0 : 0.0;
-            if (A == B) f *= 0.5;
-            if (C == D) f *= 0.5;
-            if (bra == ket) f *= 0.5;
-            const double fj = 4.0 * f, fk = 2.0 * f;
+            R f = active ? R(1) : R(0);
+            if (A == B) f *= R(0.5);
+            if (C == D) f *= R(0.5);
+            if (bra == ket) f *= R(0.5);
+            const R fj = R(4) * f, fk = R(2) * f;
+            const R ABr[3] = {R(q.AB[0]), R(q.AB[1]), R(q.AB[2])};
 
-            double jab[S::NSAB];
+            R jab[S::NSAB];
 #pragma unroll
-            for (int e = 0; e < S::NSAB; ++e) jab[e] = 0.0;
+            for (int e = 0; e < S::NSAB; ++e) jab[e] = R(0);
             if (active) {
-                double kad[CARRY ? 1 : S::NSA][CARRY ? 1 : S::NSD];
-                double kbd[S::NSB][S::NSD];
+                R kad[CARRY ? 1 : S::NSA][CARRY ? 1 : S::NSD];
+                R kbd[S::NSB][S::NSD];
                 if constexpr (!CARRY) {
 #pragma unroll
                     for (int a = 0; a < S::NSA; ++a)
@@ -505,7 +508,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                     for (int d = 0; d < S::NSD; ++d) kbd[bq][d] = 0.0;
                 sfor<S::NSC>([&](auto SC) {
                     constexpr int sc = TLNO_CI(SC);
-                    double kac[CARRY ? 1 : S::NSA], kbc[S::NSB];
+                    R kac[CARRY ? 1 : S::NSA], kbc[S::NSB];
                     if constexpr (!CARRY) {
 #pragma unroll
                         for (int a = 0; a < S::NSA; ++a) kac[a] = 0.0;
@@ -519,36 +522,36 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                         const bool own = S::BY_SC ? (sc % S::TPQ == g) : (t % S::TPQ == g);
                         if (!own) return;
                         own_sc = true;
-                        double V[S::NSAB];
+                        R V[S::NSAB];
                         sfor<S::NSA>([&](auto SA) {
                             sfor<S::NSB>([&](auto SB) {
                                 constexpr int sa = TLNO_CI(SA), sb = TLNO_CI(SB);
-                                V[sa * S::NSB + sb] = pair_transfer<LA, LB, sa, sb, S::OFA>(
-                                    q.AB, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
+                                V[sa * S::NSB + sb] = pair_transfer<R, LA, LB, sa, sb, S::OFA>(
+                                    ABr, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
                             });
                         });
                         if (cl.want_j) {
-                            double s = 0.0;
+                            R s = R(0);
 #pragma unroll
-                            for (int e = 0; e < S::NSAB; ++e) s += V[e] * dm(a0 + e / S::NSB, b0 + e % S::NSB);
+                            for (int e = 0; e < S::NSAB; ++e) s += V[e] * R(dm(a0 + e / S::NSB, b0 + e % S::NSB));
                             if constexpr (CARRY)
                                 jcd[t] += fj * s;
                             else
-                                atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, fj * s);
-                            const double dcd = dm(c0 + sc, d0 + sd);
+                                atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, double(fj * s));
+                            const R dcd = R(dm(c0 + sc, d0 + sd));
 #pragma unroll
                             for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
                         }
                         if (cl.want_k) {
 #pragma unroll
                             for (int sa = 0; sa < S::NSA; ++sa) {
-                                const double dad = dm(a0 + sa, d0 + sd), dac = dm(a0 + sa, c0 + sc);
-                                double sac = 0.0, sad = 0.0;
+                                const R dad = R(dm(a0 + sa, d0 + sd)), dac = R(dm(a0 + sa, c0 + sc));
+                                R sac = R(0), sad = R(0);
 #pragma unroll
                                 for (int sb = 0; sb < S::NSB; ++sb) {
-                                    const double v = V[sa * S::NSB + sb];
-                                    sac += v * dm(b0 + sb, d0 + sd);
-                                    sad += v * dm(b0 + sb, c0 + sc);
+                                    const R v = V[sa * S::NSB + sb];
+                                    sac += v * R(dm(b0 + sb, d0 + sd));
+                                    sad += v * R(dm(b0 + sb, c0 + sc));
                                     kbc[sb] += v * dad;
                                     kbd[sb][sd] += v * dac;
                                 }
@@ -566,11 +569,11 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                         if constexpr (!CARRY) {
 #pragma unroll
                             for (int sa = 0; sa < S::NSA; ++sa)
-                                atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, fk * kac[sa]);
+                                atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, double(fk * kac[sa]));
                         }
 #pragma unroll
                         for (int sb = 0; sb < S::NSB; ++sb)
-                            atomicAdd(Km + (long long)(b0 + sb) * M + c0 + sc, fk * kbc[sb]);
+                            atomicAdd(Km + (long long)(b0 + sb) * M + c0 + sc, double(fk * kbc[sb]));
                     }
                 });
                 if (cl.want_k) {
@@ -584,11 +587,11 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                         if constexpr (!CARRY) {
 #pragma unroll
                             for (int sa = 0; sa < S::NSA; ++sa)
-                                atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, fk * kad[sa][sd]);
+                                atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, double(fk * kad[sa][sd]));
                         }
 #pragma unroll
                         for (int sb = 0; sb < S::NSB; ++sb)
-                            atomicAdd(Km + (long long)(b0 + sb) * M + d0 + sd, fk * kbd[sb][sd]);
+                            atomicAdd(Km + (long long)(b0 + sb) * M + d0 + sd, double(fk * kbd[sb][sd]));
                     });
                 }
             }
@@ -596,10 +599,10 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                 // J[ab]: every lane of the warp shares the bra pair.
 #pragma unroll
                 for (int e = 0; e < S::NSAB; ++e) {
-                    double s = fj * jab[e];
+                    R s = fj * jab[e];
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                    if (lane == 0 && s != 0.0) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, s);
+                    if (lane == 0 && s != R(0)) atomicAdd(Jm + (long long)(a0 + e / S::NSB) * M + b0 + e % S::NSB, double(s));
                 }
             }
             if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
@@ -611,15 +614,15 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                 if (cl.want_j) {
 #pragma unroll
                     for (int t = 0; t < S::NSCD; ++t)
-                        atomicAdd(Jm + (long long)(c0 + t / S::NSD) * M + d0 + t % S::NSD, jcd[t]);
+                        atomicAdd(Jm + (long long)(c0 + t / S::NSD) * M + d0 + t % S::NSD, double(jcd[t]));
                 }
                 if (cl.want_k) {
 #pragma unroll
                     for (int sa = 0; sa < S::NSA; ++sa) {
 #pragma unroll
-                        for (int sc = 0; sc < S::NSC; ++sc) atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, kacc[sa][sc]);
+                        for (int sc = 0; sc < S::NSC; ++sc) atomicAdd(Km + (long long)(a0 + sa) * M + c0 + sc, double(kacc[sa][sc]));
 #pragma unroll
-                        for (int sd = 0; sd < S::NSD; ++sd) atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, kadc[sa][sd]);
+                        for (int sd = 0; sd < S::NSD; ++sd) atomicAdd(Km + (long long)(a0 + sa) * M + d0 + sd, double(kadc[sa][sd]));
                     }
                 }
             }

@@ -7,7 +7,8 @@ coefficients); the library normalises each Cartesian component the way the
 reference's ``make_shell`` does (core/shell/shell_contract.cpp:41-48) and
 orders the spherical AOs shell by shell (2L+1 each).
 
-Recipes (with the choices they leave open made explicit):
+Recipes of the synthetic workloads cfg0-cfg4 (the choices the workload
+descriptions leave open made explicit):
 
 * cfg0 -- water, O (0, 0, 0.117) A, H (0, +-0.757, -0.469) A.  O: s, s, p;
   each H: s; 3 primitives each; exponents log-uniform in [0.1, 200] and
