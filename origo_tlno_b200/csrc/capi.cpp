@@ -101,11 +101,11 @@ void validate_density_host(const double* D, int M) {
 // Enqueues one J/K build on stream s over device buffers.
 void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const double* dD, double* dJ,
                 double* dK, long long total, int M_single, bool want_j, bool want_k, bool mixed,
-                double* d_dmax, cudaStream_t s) {
+                double* d_dmax, float* dD32, cudaStream_t s) {
     TLNO_CUDA(cudaMemsetAsync(dJ, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(dK, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(plan.d_counters.ptr, 0, sizeof(int) * 2 * plan.combos.size(), s));
-    if (mixed) launch_absmax(dD, total, d_dmax, s);
+    if (mixed) launch_absmax_f32(dD, total, d_dmax, dD32, s);
     const dev::PlanView pv = plan.view();
     int sms = 0, devid = 0;
     TLNO_CUDA(cudaGetDevice(&devid));
@@ -127,6 +127,7 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
         cl.tau_mix = mixed_threshold;
         cl.dmax = d_dmax;
         cl.dens = dD;
+        cl.dens32 = dD32;
         cl.J = dJ;
         cl.K = dK;
         cl.M = M_single;
@@ -325,8 +326,13 @@ int tlno_gpu_jk(tlno_gpu_context* ctx, const double* density, double* J, double*
         }
         double* dJ = (dev_ptrs && J && (flags & TLNO_GPU_WANT_J)) ? J : ctx->w.J.as<double>();
         double* dK = (dev_ptrs && K && (flags & TLNO_GPU_WANT_K)) ? K : ctx->w.K.as<double>();
+        float* d32 = nullptr;
+        if (mixed) {
+            ctx->w.D32.alloc(sizeof(float) * n);
+            d32 = ctx->w.D32.as<float>();
+        }
         enqueue_jk(*ctx->plan, ctx->tune, ctx->screening.mixed_threshold, dD, dJ, dK, n, M, want_j, want_k,
-                   mixed, ctx->w.dmax.as<double>(), s);
+                   mixed, ctx->w.dmax.as<double>(), d32, s);
         if (want_g) {
             double* dG = G;
             if (!dev_ptrs) {
@@ -594,10 +600,15 @@ int tlno_gpu_jk_graph_capture(tlno_gpu_context* ctx, const double* d_density, do
         if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
         const bool want_j = (flags & (TLNO_GPU_WANT_J | TLNO_GPU_WANT_G)) || !(flags & TLNO_GPU_WANT_K);
         const bool want_k = (flags & (TLNO_GPU_WANT_K | TLNO_GPU_WANT_G)) || !(flags & TLNO_GPU_WANT_J);
+        float* d32 = nullptr;
+        if (flags & TLNO_GPU_MIXED) {  // allocated before the capture
+            ctx->w.D32.alloc(sizeof(float) * n);
+            d32 = ctx->w.D32.as<float>();
+        }
         TLNO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         try {
             enqueue_jk(*ctx->plan, ctx->tune, ctx->screening.mixed_threshold, d_density, d_J, d_K, n, M, want_j,
-                       want_k, flags & TLNO_GPU_MIXED, ctx->w.dmax.as<double>(), ctx->stream);
+                       want_k, flags & TLNO_GPU_MIXED, ctx->w.dmax.as<double>(), d32, ctx->stream);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(ctx->stream, &g);
@@ -691,6 +702,8 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int re
         cl.tile_end = cs.n_tiles;
         cl.tau = plan.tau;
         cl.dens = ctx->w.D.as<double>();
+        ctx->w.D32.alloc(sizeof(float) * n);
+        cl.dens32 = ctx->w.D32.as<float>();
         cl.J = ctx->w.J.as<double>();
         cl.K = ctx->w.K.as<double>();
         cl.M = M;
@@ -796,8 +809,13 @@ int tlno_gpu_batch_jk(tlno_gpu_batch* b, const double* density, double* J, doubl
         }
         double* dJ = dev_ptrs ? J : b->w.J.as<double>();
         double* dK = dev_ptrs ? K : b->w.K.as<double>();
+        float* d32 = nullptr;
+        if (flags & TLNO_GPU_MIXED) {
+            b->w.D32.alloc(sizeof(float) * b->total);
+            d32 = b->w.D32.as<float>();
+        }
         enqueue_jk(b->plan, b->tune, b->screening.mixed_threshold, dD, dJ, dK, b->total, 0, true, true,
-                   flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), s);
+                   flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), d32, s);
         if (!dev_ptrs) {
             TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
             TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
@@ -813,10 +831,15 @@ int tlno_gpu_batch_graph_capture(tlno_gpu_batch* b, const double* d_density, dou
         ensure_work(b->w, 1);
         if (b->graph_exec) { cudaGraphExecDestroy(b->graph_exec); b->graph_exec = nullptr; }
         if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+        float* d32 = nullptr;
+        if (flags & TLNO_GPU_MIXED) {  // allocated before the capture
+            b->w.D32.alloc(sizeof(float) * b->total);
+            d32 = b->w.D32.as<float>();
+        }
         TLNO_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         try {
             enqueue_jk(b->plan, b->tune, b->screening.mixed_threshold, d_density, d_J, d_K, b->total, 0, true, true,
-                       flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), b->stream);
+                       flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), d32, b->stream);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(b->stream, &g);

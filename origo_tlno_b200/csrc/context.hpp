@@ -18,6 +18,7 @@ void set_last_error(const std::string& message);
 
 struct JkWork {
     DeviceBuffer D, J, K, G, dmax, status;
+    DeviceBuffer D32;  // FP32 copy of the density for the FP32 kernels (mixed builds)
 };
 }  // namespace tlno_gpu
 

@@ -430,7 +430,14 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         const double* Dm = cl.dens + mbase;
         double* Jm = cl.J + mbase;
         double* Km = cl.K + mbase;
-        auto dm = [&](int r, int c) { return __ldg(Dm + (long long)r * M + c); };
+        // FP32 kernels gather from the FP32 copy of the density
+        const float* Dm32 = cl.dens32 + mbase;
+        auto dm = [&](int r, int c) {
+            if constexpr (std::is_same<R, float>::value)
+                return R(__ldg(Dm32 + (long long)r * M + c));
+            else
+                return __ldg(Dm + (long long)r * M + c);
+        };
         const int c0 = __ldg(pv.shell_sph + C), d0 = __ldg(pv.shell_sph + D);
 
         // Sums carried across the bras of a block (they share the first

@@ -191,6 +191,27 @@ __global__ void absmax_kernel(const double* x, long long n, double* out) {
     }
 }
 
+// max|x| as above, and x rounded to FP32 (the density copy the FP32
+// kernels of a mixed build gather from) in the same pass.
+__global__ void absmax_f32_kernel(const double* x, long long n, double* out, float* x32) {
+    __shared__ double red[32];
+    double m = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double v = x[e];
+        x32[e] = static_cast<float>(v);
+        m = fmax(m, fabs(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0)
+            atomicMax(reinterpret_cast<unsigned long long*>(out), static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
 __global__ void validate_density_kernel(const double* D, int M, unsigned int* status) {
     const long long n = (long long)M * M;
     unsigned int bits = 0;
@@ -423,6 +444,13 @@ void launch_absmax(const double* x, long long n, double* out, cudaStream_t s) {
     TLNO_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
     const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 1023) / 1024, sm_count() * 4)));
     absmax_kernel<<<grid, 1024, 0, s>>>(x, n, out);
+    TLNO_CUDA(cudaGetLastError());
+}
+
+void launch_absmax_f32(const double* x, long long n, double* out, float* x32, cudaStream_t s) {
+    TLNO_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 1023) / 1024, sm_count() * 4)));
+    absmax_f32_kernel<<<grid, 1024, 0, s>>>(x, n, out, x32);
     TLNO_CUDA(cudaGetLastError());
 }
 

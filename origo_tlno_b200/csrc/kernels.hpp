@@ -38,6 +38,8 @@ void launch_symmetrize(double* X, const long long* offsets, const int* dims, int
 void launch_symmetrize_single(double* X, int M, cudaStream_t s);
 // *out = max |x_i| over n elements.
 void launch_absmax(const double* x, long long n, double* out, cudaStream_t s);
+// max|x| into *out and the FP32 copy x32 of x, one pass.
+void launch_absmax_f32(const double* x, long long n, double* out, float* x32, cudaStream_t s);
 // Density contract check: bit 1 = non-finite entry, bit 2 = asymmetric
 // beyond 128 eps * max(1, |Dij|, |Dji|) (direct_build.ipp:25-96).
 void launch_validate_density(const double* D, int M, unsigned int* status, cudaStream_t s);

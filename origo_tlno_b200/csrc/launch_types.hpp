@@ -73,6 +73,7 @@ struct ClassLaunch {
     double* out;                  // STORE: blocks; SCHWARZ: Q per quartet
     const long long* out_off;     // STORE: element offset per quartet
     const double* dens;
+    const float* dens32;          // FP32 copy of dens (FP32 kernels of a mixed build)
     double* J;
     double* K;
     int M;                        // single-molecule AO count (when no batch)
