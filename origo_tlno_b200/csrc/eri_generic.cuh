@@ -128,10 +128,12 @@ __device__ __forceinline__ void build_pair_projector(double* Pm, int la, int lb,
     }
 }
 
+// build_pb = false reuses the bra projector this warp built for the same
+// bra pair (it lives in its own region of the warp's shared memory).
 template <typename R, int MODE>
 __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
                                 const GenericLayout& lay, double* wsm, int lane,
-                                int bra, int ket, int quartet_id) {
+                                int bra, int ket, int quartet_id, bool build_pb = true) {
     const int A = pv.pair_A[bra], B = pv.pair_B[bra];
     const int C = pv.pair_A[ket], D = pv.pair_B[ket];
     const double* xa = pv.shell_xyz + 3 * A;
@@ -201,7 +203,7 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
     // HRR + spherical projection: V = PB * T * PK^T.
     double* PB = wsm + lay.off_PB;
     double* PK = wsm + lay.off_PK;
-    build_pair_projector(PB, la, lb, xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2], lane);
+    if (build_pb) build_pair_projector(PB, la, lb, xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2], lane);
     build_pair_projector(PK, lc, ld, xc[0] - xd[0], xc[1] - xd[1], xc[2] - xd[2], lane);
     __syncwarp();
     double* X = wsm + lay.off_X;
@@ -340,6 +342,7 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double* wsm = smem + warp * lay.words;
     const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
+    int pb_bra = -1;  // bra pair whose projector this warp holds
     for (int tile = cl.tile_begin + blockIdx.x; tile < cl.tile_end; tile += gridDim.x) {
         const int b = find_block(cl.tile_prefix, cl.n_blocks, tile);
         const int kb = tile - __ldg(cl.tile_prefix + b);
@@ -356,7 +359,8 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
             if (!(qq >= cl.tau)) continue;
             if (cl.prec_mode == 1 && !(qq >= thr)) continue;
             if (cl.prec_mode == 2 && qq >= thr) continue;
-            generic_quartet<R, kJK>(pv, cl, lay, wsm, lane, bra, ket, 0);
+            generic_quartet<R, kJK>(pv, cl, lay, wsm, lane, bra, ket, 0, bra != pb_bra);
+            pb_bra = bra;
         }
     }
 }
