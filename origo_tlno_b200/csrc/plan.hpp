@@ -13,7 +13,7 @@ namespace tlno_gpu {
 
 struct Tuning {
     int fast_bb = 4;        // accepted and ignored (compile-time kernels take one bra per tile)
-    int generic_bk = 16;    // ket pairs per tile of the warp-per-quartet kernel
+    int generic_bk = 64;    // ket pairs per tile of the warp-per-quartet kernel
     int generic_warps = 0;  // 0 = from shared-memory budget
     int grid_mult = 8;      // CTAs per SM for persistent launches
     std::array<int, 256> force_generic{};  // per class combo: 1 = never use the fast kernel

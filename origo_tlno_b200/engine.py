@@ -197,7 +197,7 @@ class Context:
         N.check(N.lib().tlno_gpu_set_onee_thresholds(self.h, decay_eps, nuclear_eps))
 
     # -- tuning ---------------------------------------------------------
-    def set_tuning(self, fast_bb=4, generic_bk=16, generic_warps=0, grid_mult=8):
+    def set_tuning(self, fast_bb=4, generic_bk=64, generic_warps=0, grid_mult=8):
         t = N.Tuning(fast_bb, generic_bk, generic_warps, grid_mult)
         N.check(N.lib().tlno_gpu_set_tuning(self.h, C.byref(t)))
 
