@@ -37,7 +37,7 @@ def main(argv=None) -> int:
     ap.add_argument("workload", help="cfg0..cfg4 or waterN")
     ap.add_argument("--classes", default="", help='comma-separated class tags such as "10|00,11|10"')
     ap.add_argument("--reps", type=int, default=2)
-    ap.add_argument("--fp32", action="store_true", help="also time the FP32 kernel of each class")
+    ap.add_argument("--fp32", action="store_true", help="also time the FP32 kernel of each class (with --once: launch only the FP32 kernel)")
     ap.add_argument("--eri-only", action="store_true", help="also time the class without J/K digestion")
     ap.add_argument("--once", action="store_true", help="launch each selected class once, no timing loop")
     ap.add_argument("--plan-only", action="store_true")
@@ -59,6 +59,10 @@ def main(argv=None) -> int:
                "flops_model": c["flops"]}
         if not a.plan_only:
             reps = 0 if a.once else a.reps
+            if a.once and a.fp32:  # launch the FP32 kernel only
+                row["ms_fp32"] = ctx.time_combo(i, fp32=True, reps=0)
+                print(json.dumps(row), flush=True)
+                continue
             ms = ctx.time_combo(i, reps=reps)
             row["ms_fp64"] = ms
             if not a.once:
