@@ -285,7 +285,8 @@ def run_batch(args):
            "batched_speedup_vs_one_context_per_molecule": seq / (t64 / args.steps),
            "accuracy": {"max_abs_dJ": float((Jmx - J64).abs().max()), "max_abs_dK": float((Kmx - K64).abs().max())},
            "gpu_launches": None}
-    print(json.dumps(res))
+    if rank == 0:
+        print(json.dumps(res))
     return 0
 
 
