@@ -138,6 +138,19 @@ def test_cfg2_fragment_f_shells():
     ctx.close()
 
 
+def test_plan_counts_surviving_quartets_exactly(ctx1):
+    # the plan's quartet count (the bench's quartets/s numerator) equals a
+    # brute-force count of unordered shell-pair pairs {P, Q} (P = Q included)
+    # with Q_P Q_Q >= tau over the library's own Schwarz bounds
+    tau = 1e-12
+    q = ctx1.schwarz()
+    n = 0
+    for i in range(len(q)):
+        # partners j >= i, each unordered pair once, same product test as the plan
+        n += int(np.count_nonzero(q[i] * q[i:] >= tau))
+    assert ctx1.profile()["quartets"] == n
+
+
 def test_mixed_threshold_autotune_cfg1():
     # the autotuner keeps the largest split threshold whose mixed build stays
     # within its tolerances of the FP64 build, and sets it on the context
