@@ -46,13 +46,29 @@ extern "C" {
 typedef struct tlno_gpu_context tlno_gpu_context;
 
 /* Screening options; field meaning of the reference's
- * fock::ScreeningOptions (integrals/two_electron/fock/jk_direct.hpp:18-24)
- * plus the mixed-precision split threshold. */
+ * fock::ScreeningOptions (integrals/two_electron/fock/jk_direct.hpp:18-24,
+ * twoe_integrals.hpp:43-66) plus the mixed-precision split threshold.
+ *   integral_threshold: Schwarz, keep shell quartets with Q_ab Q_cd >= tau.
+ *   primitive_fastschwarz_threshold t: drop primitive quartets whose Simint
+ *     FASTSCHWARZ estimate product is below t^2 (classes up to f); the
+ *     reference drops a SIMD packet of primitive quartets only when all of
+ *     its lanes fail, this engine drops each failing primitive quartet.
+ *   decay_threshold: the heuristic shell-pair decay indicator
+ *     K_A K_B exp(-mu |AB|^2) replaces the Schwarz bound as the pair metric;
+ *     the reference's specialised route requires integral_threshold == 0
+ *     with it, and so does this engine (same error text).
+ *   density_threshold: CVHF density screen, q * max(4 max(rho_ab, rho_cd),
+ *     max(rho_ac, rho_ad, rho_bc, rho_bd)) >= threshold with rho the
+ *     shell-block maxima of |D| and the raised cutoff
+ *     q >= max(tau, threshold / (4 max|D|)) (direct_build.ipp:122-251); J
+ *     uses the Coulomb cap, K the exchange cap (with threshold / max|D|), G
+ *     the larger of the two, as build_coulomb_j / build_exchange_k /
+ *     build_rhf_g do.  Cannot be combined with decay_threshold. */
 typedef struct {
-    double integral_threshold;             /* Schwarz: keep Q_ab Q_cd >= tau */
-    double primitive_fastschwarz_threshold; /* accepted; must be 0 (not used) */
-    double decay_threshold;                 /* accepted; must be 0 (not used) */
-    double density_threshold;               /* accepted; must be 0 (not used) */
+    double integral_threshold;
+    double primitive_fastschwarz_threshold;
+    double decay_threshold;
+    double density_threshold;
     double mixed_threshold;                 /* FP32 when Q_ab Q_cd max|D| < this */
 } tlno_gpu_screening;
 
@@ -121,6 +137,79 @@ int tlno_gpu_plan_profile(const tlno_gpu_context* ctx, tlno_gpu_profile* out);
 int tlno_gpu_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, double* G,
                 int flags);
 
+/* tlno_gpu_jk with the build-time screening options of the reference's
+ * calls build_coulomb_j(plan, density, options) and its siblings
+ * (jk_direct.hpp:82-96), which take the options again at build time:
+ * density and primitive FASTSCHWARZ screening apply to this build; an
+ * integral_threshold or decay_threshold other than the plan's re-plans
+ * first (the options become the context's).  With TLNO_GPU_WANT_G alone it
+ * is also the compatibility entry build_jk_direct_for_G_rys(plan, density,
+ * options) (fock/eri_direct_jk.hpp:36-39): G = J - K/2 under the fused
+ * density predicate.  mixed_threshold keeps the context's value. */
+int tlno_gpu_jk_with_options(tlno_gpu_context* ctx, const double* density, double* J, double* K,
+                             double* G, int flags, const tlno_gpu_screening* options);
+
+/* ERI checksum stream: the sum of every canonical unique spherical ERI
+ * (ij|kl), i >= j, k >= l, ij >= kl over AO pair indices, whose shell
+ * quartet passes the plan's shell-level screen -- the value
+ * build_eri_packed_for_G_rys returns in streaming mode
+ * (integrals/two_electron/twoe_integrals.hpp:114-119, rys_engine.ipp:
+ * 269-274, 690-708), and the ERI-only throughput endpoint timed by
+ * benchmarks/two_electron_engine/src/twoe_timing.cpp.  FP64.  Requires a
+ * plan; *ms (may be null) receives the device time of the kernels. */
+int tlno_gpu_eri_checksum(tlno_gpu_context* ctx, double* checksum, double* ms);
+
+/* Incremental (dP) RHF G builds for SCF iterations: the reference's
+ * EriDirectJKIncrementalState (integrals/two_electron/fock/
+ * eri_direct_jk.hpp:41-135, direct_build.ipp:562-775).  The first density,
+ * every forced rebuild and every exact_rebuild_interval-th changed density
+ * rebuild G = J - K/2 from the full density with density screening off;
+ * the updates between contract dP = D - D_prev under
+ * delta_density_threshold (or first_delta_density_threshold for the first
+ * changed update after a rebuild when use_first_delta_density_threshold is
+ * set) and add dG to the cached G.  An unchanged density is skipped.
+ * Strong guarantee: a failed update leaves density, G, cadence, counters
+ * and diagnostics as they were.  D and G live on the context's device. */
+typedef struct tlno_gpu_incremental tlno_gpu_incremental;
+typedef struct {
+    tlno_gpu_screening base_options;        /* density_threshold is forced to 0 */
+    unsigned long long exact_rebuild_interval; /* >= 1 */
+    double delta_density_threshold;
+    int use_first_delta_density_threshold;
+    double first_delta_density_threshold;
+} tlno_gpu_incremental_options;
+#define TLNO_GPU_UPDATE_EXACT 1
+#define TLNO_GPU_UPDATE_INCREMENTAL 2
+#define TLNO_GPU_UPDATE_SKIPPED 3
+typedef struct {
+    unsigned long long updates, exact_rebuilds, incremental_updates, skipped_updates;
+    int last_status;                        /* 0 before the first update */
+    int initialized;
+    double last_max_abs_density_delta;
+    double last_effective_density_threshold;
+    unsigned long long updates_since_exact_rebuild;
+} tlno_gpu_incremental_info;
+/* The state keeps a plan of its own built from options->base_options. */
+int tlno_gpu_incremental_create(tlno_gpu_context* ctx, const tlno_gpu_incremental_options* options,
+                                tlno_gpu_incremental** out);
+void tlno_gpu_incremental_destroy(tlno_gpu_incremental* st);
+/* Returns TLNO_GPU_UPDATE_* (>= 1) or a negative status.  flags:
+ * TLNO_GPU_DEVICE_PTRS (density on the device), TLNO_GPU_MIXED (mixed
+ * precision builds). */
+int tlno_gpu_incremental_update(tlno_gpu_incremental* st, const double* density, int force_exact_rebuild,
+                                int flags);
+/* Copies the cached G (or the cached density) to G (host, or device with
+ * TLNO_GPU_DEVICE_PTRS). */
+int tlno_gpu_incremental_g(const tlno_gpu_incremental* st, double* G, int flags);
+int tlno_gpu_incremental_density(const tlno_gpu_incremental* st, double* D, int flags);
+int tlno_gpu_incremental_info_get(const tlno_gpu_incremental* st, tlno_gpu_incremental_info* out);
+/* Back to the just-created state (plan and options kept). */
+int tlno_gpu_incremental_reset(tlno_gpu_incremental* st);
+/* Testing hook for the strong guarantee: the next update fails with
+ * TLNO_GPU_E_STATE at `stage` (1 = after validation, before the build;
+ * 2 = after the build, before the commit); 0 clears it. */
+int tlno_gpu_incremental_fail_next_update(tlno_gpu_incremental* st, int stage);
+
 /* One-electron S, T, V (spherical, M x M).  screening != 0 applies the
  * reference's default screening (group-pair decay 1e-15, nuclear primitive
  * 1e-15 / sum|Z|); 0 disables it.  Replaces
@@ -147,7 +236,10 @@ int tlno_gpu_eri_blocks(tlno_gpu_context* ctx, int n_quartets, const int* shells
                         const long long* offsets, double* out);
 
 /* The same ERI blocks as tlno_gpu_eri_blocks, without any device
- * allocation: no cudaMalloc, cudaFree or allocating library call.  For
+ * allocation: no cudaMalloc, cudaFree or allocating library call.  The call
+ * blocks until its copy and kernels have finished (it synchronises the
+ * context's stream); work the caller queued on other streams that touches
+ * d_out must be finished before the call.  For
  * callers that cannot allocate device memory -- code that works inside a
  * device-memory budget owned by another allocator (a framework's pool), on a
  * latency-critical path where an allocation may synchronise the device, or
@@ -156,12 +248,12 @@ int tlno_gpu_eri_blocks(tlno_gpu_context* ctx, int n_quartets, const int* shells
  * d_out is caller-owned device memory of the context's device; block q is
  * written at d_out + offsets[q] (element offsets, host array); shells4 is a
  * host array.  Per-call scratch (pair tables, primitive pairs, quartet lists)
- * lives in one fixed 8 MiB device array that every device loading the
- * library holds until exit; a request needing more fails with
- * TLNO_GPU_E_INVALID and a message naming the sizes (split it).  The first
- * call on a device looks up that array's address (cudaGetSymbolAddress), so
- * it should come before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (e.g. from two host threads) race. */
+ * lives in one fixed 8 MiB device array that every device on which a
+ * context is created holds until exit (context creation looks up its
+ * address with cudaGetSymbolAddress, which loads it); a request needing more
+ * fails with TLNO_GPU_E_INVALID and a message naming the sizes (split it).
+ * All calls share the array: calls that overlap on the GPU (e.g. from two
+ * host threads) race. */
 int tlno_gpu_eri_blocks_noalloc(tlno_gpu_context* ctx, int n_quartets, const int* shells4,
                                 const long long* offsets, double* d_out);
 
@@ -213,13 +305,12 @@ int tlno_gpu_batch_graph_launch(tlno_gpu_batch* b);
 int tlno_gpu_batch_synchronize(tlno_gpu_batch* b);
 void* tlno_gpu_batch_stream(tlno_gpu_batch* b);
 
-/* Tuning of the kernel schedule: fast_bb is accepted (1..4) and ignored
- * (the compile-time kernels take one bra pair per tile and size their grid
- * from the occupancy calculator, capped by grid_mult x SMs);
- * generic-kernel ket tile, generic warps per CTA, persistent grid
- * multiplier; and a per-class-combination generic override. */
+/* Tuning of the kernel schedule: generic-kernel ket tile, generic warps
+ * per CTA (0 = from the shared-memory budget), persistent grid multiplier
+ * (the compile-time kernels size their grid from the occupancy calculator,
+ * capped by grid_mult x SMs); and a per-class-combination generic
+ * override. */
 typedef struct {
-    int fast_bb;
     int generic_bk;
     int generic_warps;
     int grid_mult;

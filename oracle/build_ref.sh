@@ -8,10 +8,11 @@
 # reference's AVX2 "Release" options (CMakeLists.txt:9-34: -march=x86-64-v3,
 # -O3 -DNDEBUG, OpenMP, C++17).  Output goes only to oracle/_ref/.
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   reference_root defaults to $TLNO_REFERENCE_ROOT, then /root/reference.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${TLNO_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"
 # The image may export CXX pointing at a compiler without libgomp; the
@@ -51,3 +52,13 @@ fi
 for p in "${pids[@]}"; do wait "$p"; done
 "$CXX" -shared -fopenmp -o "$OUT/libtlno_ref.so" "${objs[@]}"
 echo "build_ref: wrote $OUT/libtlno_ref.so"
+# The C++ shim test (tests/shim/shim_test.cpp) compiled against the
+# reference's headers, linking the compiled reference and the engine library
+# (built before this script runs).
+ROOT="$(cd "$HERE/.." && pwd)"
+GPU_LIB="$ROOT/origo_tlno_b200/_lib"
+if [ -f "$GPU_LIB/libtlno_gpu.so" ]; then
+  "$CXX" -std=c++17 -O2 -fopenmp -I"$REF" -I"$ROOT" -w "$ROOT/tests/shim/shim_test.cpp" -o "$OUT/shim_test" \
+    -L"$OUT" -ltlno_ref -L"$GPU_LIB" -ltlno_gpu -Wl,-rpath,'$ORIGIN' -Wl,-rpath,'$ORIGIN/../../origo_tlno_b200/_lib'
+  echo "build_ref: wrote $OUT/shim_test"
+fi

@@ -77,6 +77,14 @@ def lib():
         L.ref_boys_hgp.argtypes = [C.c_int, C.c_double]
         L.ref_rys_roots.argtypes = [C.c_int, C.c_double, vp, vp]
         L.ref_rys_roots_accurate.argtypes = [C.c_int, C.c_double, vp, vp]
+        L.ref_jk_opts.argtypes = [vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, vp, vp, vp]
+        L.ref_jk_compat.argtypes = [vp, vp, C.c_double, C.c_double, vp]
+        L.ref_eri_checksum.argtypes = [vp, C.c_double, vp, vp]
+        L.ref_incremental_create.restype = vp
+        L.ref_incremental_create.argtypes = [vp, C.c_double, C.c_ulonglong, C.c_double, C.c_int, C.c_double]
+        L.ref_incremental_destroy.argtypes = [vp]
+        L.ref_incremental_update.argtypes = [vp, vp, C.c_int, vp, vp, vp, vp, vp]
+        L.ref_basis_components.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -130,6 +138,51 @@ class RefBasis:
                               out["G"].ctypes.data if "G" in out else None))
         return out
 
+    def jk_opts(self, D, schwarz=1e-12, fastschwarz=0.0, decay=0.0, density_threshold=0.0,
+                want=("J", "K", "G")):
+        """J / K / G through the public facade with every ScreeningOptions field."""
+        M = self.M
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        out = {k: np.empty((M, M)) for k in want}
+        with single_thread():
+            _chk(lib().ref_jk_opts(self.h, D.ctypes.data, schwarz, fastschwarz, decay, density_threshold,
+                                   out["J"].ctypes.data if "J" in out else None,
+                                   out["K"].ctypes.data if "K" in out else None,
+                                   out["G"].ctypes.data if "G" in out else None))
+        return out
+
+    def jk_compat(self, D, schwarz=1e-12, density_threshold=0.0):
+        """G through build_jk_direct_for_G_rys (the compatibility endpoint)."""
+        M = self.M
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        G = np.empty((M, M))
+        with single_thread():
+            _chk(lib().ref_jk_compat(self.h, D.ctypes.data, schwarz, density_threshold, G.ctypes.data))
+        return G
+
+    def eri_checksum(self, schwarz=0.0):
+        """(checksum, seconds) of the ERI stream endpoint."""
+        cs = C.c_double()
+        t = C.c_double()
+        with single_thread():
+            _chk(lib().ref_eri_checksum(self.h, schwarz, C.byref(cs), C.byref(t)))
+        return cs.value, t.value
+
+    def components(self):
+        """Per-Cartesian-component records (centers, ang, nprim, exps, coefs)
+        exactly as the reference holds its std::vector<Shell>."""
+        nc = C.c_int()
+        npr = C.c_int()
+        _chk(lib().ref_basis_components(self.h, C.byref(nc), C.byref(npr), None, None, None, None, None))
+        centers = np.empty((nc.value, 3))
+        ang = np.empty((nc.value, 3), dtype=np.int32)
+        nprim = np.empty(nc.value, dtype=np.int32)
+        exps = np.empty(npr.value)
+        coefs = np.empty(npr.value)
+        _chk(lib().ref_basis_components(self.h, C.byref(nc), C.byref(npr), centers.ctypes.data, ang.ctypes.data,
+                                        nprim.ctypes.data, exps.ctypes.data, coefs.ctypes.data))
+        return centers, ang, nprim, exps, coefs
+
     def time_jk(self, D, schwarz=1e-12, reps=1):
         D = np.ascontiguousarray(D, dtype=np.float64)
         t = np.empty(reps)
@@ -167,3 +220,43 @@ def rys_roots(n: int, t: float, accurate: bool = False):
     f = lib().ref_rys_roots_accurate if accurate else lib().ref_rys_roots
     f(n, t, r.ctypes.data, w.ctypes.data)
     return r, w
+
+
+class RefIncremental:
+    """EriDirectJKIncrementalState of the reference on its own plan."""
+
+    STATUS = {1: "exact_rebuild", 2: "incremental_update", 3: "skipped_unchanged"}
+
+    def __init__(self, basis: RefBasis, schwarz=1e-12, exact_rebuild_interval=8, delta_density_threshold=0.0,
+                 use_first_delta_density_threshold=False, first_delta_density_threshold=0.0):
+        self.basis = basis
+        self.h = lib().ref_incremental_create(basis.h, schwarz, exact_rebuild_interval, delta_density_threshold,
+                                              1 if use_first_delta_density_threshold else 0,
+                                              first_delta_density_threshold)
+        if not self.h:
+            raise RuntimeError("reference: " + lib().ref_last_error().decode())
+
+    def update(self, D, force=False):
+        M = self.basis.M
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        G = np.empty((M, M))
+        st = C.c_int()
+        cnt = np.zeros(4, dtype=np.uint64)
+        ld = C.c_double()
+        lt = C.c_double()
+        with single_thread():
+            _chk(lib().ref_incremental_update(self.h, D.ctypes.data, 1 if force else 0, G.ctypes.data, C.byref(st),
+                                              cnt.ctypes.data, C.byref(ld), C.byref(lt)))
+        return {"status": self.STATUS.get(st.value, st.value), "G": G, "counters": [int(x) for x in cnt],
+                "last_max_abs_density_delta": ld.value, "last_effective_density_threshold": lt.value}
+
+    def close(self):
+        if self.h:
+            lib().ref_incremental_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -26,10 +26,12 @@
 #include "core/math/general_math.hpp"
 #include "core/shell/shell_contract.hpp"
 #include "integrals/one_electron/onee_matrices.hpp"
+#include "integrals/two_electron/fock/eri_direct_jk.hpp"
 #include "integrals/two_electron/fock/jk_direct.hpp"
 
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 
 using namespace tlno::integrals::twoe;
@@ -193,6 +195,160 @@ int ref_jk(void* h, const double* density, double schwarz_threshold,
         if (G) {
             const auto r = fock::build_rhf_g(plan, d, opt);
             std::memcpy(G, r.g.data(), m * m * sizeof(double));
+        }
+    });
+}
+
+// J, K and G with every field of the reference's fock::ScreeningOptions
+// (fock/jk_direct.hpp:18-24): the plan is built with the same options and
+// each endpoint receives them, as a caller of the public facade does.
+int ref_jk_opts(void* h, const double* density, double schwarz_threshold,
+                double primitive_fastschwarz_threshold, double decay_threshold,
+                double density_threshold, double* J, double* K, double* G) {
+    return guarded([&] {
+        namespace fock = tlno::integrals::twoe::fock;
+        auto* rb = static_cast<RefBasis*>(h);
+        fock::ScreeningOptions opt;
+        opt.integral_threshold = schwarz_threshold;
+        opt.primitive_fastschwarz_threshold = primitive_fastschwarz_threshold;
+        opt.decay_threshold = decay_threshold;
+        opt.density_threshold = density_threshold;
+        const fock::DirectPlan plan = fock::build_direct_plan(rb->build.basis, opt);
+        const std::size_t m = static_cast<std::size_t>(plan.profile.M);
+        std::vector<double> d(density, density + m * m);
+        if (J) {
+            const auto r = fock::build_coulomb_j(plan, d, opt);
+            std::memcpy(J, r.j.data(), m * m * sizeof(double));
+        }
+        if (K) {
+            const auto r = fock::build_exchange_k(plan, d, opt);
+            std::memcpy(K, r.k.data(), m * m * sizeof(double));
+        }
+        if (G) {
+            const auto r = fock::build_rhf_g(plan, d, opt);
+            std::memcpy(G, r.g.data(), m * m * sizeof(double));
+        }
+    });
+}
+
+// G = J - K/2 through the compatibility endpoint build_jk_direct_for_G_rys
+// (fock/eri_direct_jk.hpp:36-39) on an EriPackedPlan.
+int ref_jk_compat(void* h, const double* density, double schwarz_threshold,
+                  double density_threshold, double* G) {
+    return guarded([&] {
+        auto* rb = static_cast<RefBasis*>(h);
+        EriPackedBuildOptions opt;
+        opt.schwarz_threshold = schwarz_threshold;
+        opt.density_threshold = density_threshold;
+        const EriPackedPlan plan = build_eri_packed_plan_for_G_rys(rb->build.basis, opt);
+        const std::size_t m = static_cast<std::size_t>(plan.profile.M);
+        std::vector<double> d(density, density + m * m);
+        const auto r = build_jk_direct_for_G_rys(plan, d, opt);
+        std::memcpy(G, r.g.data(), m * m * sizeof(double));
+    });
+}
+
+// ERI checksum stream (build_eri_packed_for_G_rys, twoe_integrals.hpp:117,
+// the endpoint benchmarks/two_electron_engine/src/twoe_timing.cpp times):
+// the sum of every canonical unique spherical ERI that survives the screen.
+// Also returns the plan's profile counters.
+int ref_eri_checksum(void* h, double schwarz_threshold, double* checksum,
+                     double* seconds) {
+    return guarded([&] {
+        auto* rb = static_cast<RefBasis*>(h);
+        EriPackedBuildOptions opt;
+        opt.schwarz_threshold = schwarz_threshold;
+        const EriPackedPlan plan = build_eri_packed_plan_for_G_rys(rb->build.basis, opt);
+        const auto t0 = std::chrono::steady_clock::now();
+        const EriPackedGData r = build_eri_packed_for_G_rys(plan, opt);
+        const auto t1 = std::chrono::steady_clock::now();
+        if (r.values.size() != 1) throw std::runtime_error("expected one ERI checksum");
+        *checksum = r.values.front();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    });
+}
+
+// EriDirectJKIncrementalState (fock/eri_direct_jk.hpp:41-135) over the
+// reference's own plan.
+struct RefIncremental {
+    std::unique_ptr<EriDirectJKIncrementalState> state;
+};
+
+void* ref_incremental_create(void* h, double schwarz_threshold,
+                             unsigned long long exact_rebuild_interval,
+                             double delta_density_threshold,
+                             int use_first_delta_density_threshold,
+                             double first_delta_density_threshold) {
+    RefIncremental* out = nullptr;
+    const int rc = guarded([&] {
+        auto* rb = static_cast<RefBasis*>(h);
+        EriDirectJKIncrementalOptions o;
+        o.base_options.schwarz_threshold = schwarz_threshold;
+        o.exact_rebuild_interval = exact_rebuild_interval;
+        o.delta_density_threshold = delta_density_threshold;
+        o.use_first_delta_density_threshold = use_first_delta_density_threshold != 0;
+        o.first_delta_density_threshold = first_delta_density_threshold;
+        const EriPackedPlan plan =
+            build_eri_packed_plan_for_G_rys(rb->build.basis, o.base_options);
+        auto st = std::make_unique<RefIncremental>();
+        st->state = std::make_unique<EriDirectJKIncrementalState>(plan, o);
+        out = st.release();
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+void ref_incremental_destroy(void* s) { delete static_cast<RefIncremental*>(s); }
+
+// One update; writes the cached G (M x M), the status (1 exact rebuild,
+// 2 incremental update, 3 skipped unchanged) and the counters
+// [updates, exact_rebuilds, incremental_updates, skipped_updates].
+int ref_incremental_update(void* s, const double* density, int force, double* G,
+                           int* status, unsigned long long* counters,
+                           double* last_delta, double* last_threshold) {
+    return guarded([&] {
+        auto* st = static_cast<RefIncremental*>(s);
+        const std::size_t m = static_cast<std::size_t>(st->state->M());
+        std::vector<double> d(density, density + m * m);
+        const auto r = st->state->update(d, force != 0);
+        *status = static_cast<int>(r);
+        const auto& g = st->state->g();
+        std::memcpy(G, g.data(), m * m * sizeof(double));
+        const auto& c = st->state->counters();
+        counters[0] = c.updates;
+        counters[1] = c.exact_rebuilds;
+        counters[2] = c.incremental_updates;
+        counters[3] = c.skipped_updates;
+        *last_delta = st->state->last_max_abs_density_delta();
+        *last_threshold = st->state->last_effective_density_threshold();
+    });
+}
+
+// The per-Cartesian-component records of the basis exactly as the reference
+// holds them (std::vector<Shell>, core/basis/types.hpp:30-35): centre,
+// angular triple, primitive count and the make_shell-normalised primitives
+// (exponents and coefficients packed back to back).  Call with null arrays to
+// get the component and primitive counts.
+int ref_basis_components(void* h, int* n_components, int* n_prims, double* centers,
+                         int* ang, int* nprim, double* exps, double* coefs) {
+    return guarded([&] {
+        const auto& b = static_cast<RefBasis*>(h)->build.basis;
+        *n_components = static_cast<int>(b.size());
+        int np = 0;
+        for (const auto& s : b) np += static_cast<int>(s.primitives.size());
+        *n_prims = np;
+        if (!centers) return;
+        int p = 0;
+        for (std::size_t k = 0; k < b.size(); ++k) {
+            for (int a = 0; a < 3; ++a) {
+                centers[3 * k + a] = b[k].center[a];
+                ang[3 * k + a] = b[k].ang[a];
+            }
+            nprim[k] = static_cast<int>(b[k].primitives.size());
+            for (const auto& pr : b[k].primitives) {
+                exps[p] = pr.exponent;
+                coefs[p] = pr.coefficient;
+                ++p;
+            }
         }
     });
 }

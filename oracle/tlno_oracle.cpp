@@ -27,7 +27,7 @@
 //   * J/K digestion (full 8-fold sum)  fock/detail/consumer_policies.ipp:87-221
 //   * one-electron S, T, V ........... integrals/one_electron/
 //                                      onee_integrals.cpp:32-157, 284-887
-// Parity is pinned by tests/test_oracle_cpu.py against the compiled reference
+// Parity is pinned by tests/test_cpu.py against the compiled reference
 // (oracle/_ref) and the golden fixtures in tests/golden/.
 #include <algorithm>
 #include <array>

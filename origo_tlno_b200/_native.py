@@ -49,9 +49,22 @@ class Profile(C.Structure):
                 ("n_class_launches", C.c_int)]
 
 
+class IncrementalOptions(C.Structure):
+    _fields_ = [("base_options", Screening), ("exact_rebuild_interval", C.c_ulonglong),
+                ("delta_density_threshold", C.c_double), ("use_first_delta_density_threshold", C.c_int),
+                ("first_delta_density_threshold", C.c_double)]
+
+
+class IncrementalInfo(C.Structure):
+    _fields_ = [("updates", C.c_ulonglong), ("exact_rebuilds", C.c_ulonglong),
+                ("incremental_updates", C.c_ulonglong), ("skipped_updates", C.c_ulonglong),
+                ("last_status", C.c_int), ("initialized", C.c_int),
+                ("last_max_abs_density_delta", C.c_double), ("last_effective_density_threshold", C.c_double),
+                ("updates_since_exact_rebuild", C.c_ulonglong)]
+
+
 class Tuning(C.Structure):
-    _fields_ = [("fast_bb", C.c_int), ("generic_bk", C.c_int), ("generic_warps", C.c_int),
-                ("grid_mult", C.c_int)]
+    _fields_ = [("generic_bk", C.c_int), ("generic_warps", C.c_int), ("grid_mult", C.c_int)]
 
 
 _lib = None
@@ -82,6 +95,16 @@ def lib() -> C.CDLL:
         "tlno_gpu_plan": (C.c_int, [_vp, C.POINTER(Screening)]),
         "tlno_gpu_plan_profile": (C.c_int, [_vp, C.POINTER(Profile)]),
         "tlno_gpu_jk": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
+        "tlno_gpu_jk_with_options": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(Screening)]),
+        "tlno_gpu_eri_checksum": (C.c_int, [_vp, _dp, _dp]),
+        "tlno_gpu_incremental_create": (C.c_int, [_vp, C.POINTER(IncrementalOptions), C.POINTER(_vp)]),
+        "tlno_gpu_incremental_destroy": (None, [_vp]),
+        "tlno_gpu_incremental_update": (C.c_int, [_vp, _vp, C.c_int, C.c_int]),
+        "tlno_gpu_incremental_g": (C.c_int, [_vp, _vp, C.c_int]),
+        "tlno_gpu_incremental_density": (C.c_int, [_vp, _vp, C.c_int]),
+        "tlno_gpu_incremental_info_get": (C.c_int, [_vp, C.POINTER(IncrementalInfo)]),
+        "tlno_gpu_incremental_reset": (C.c_int, [_vp]),
+        "tlno_gpu_incremental_fail_next_update": (C.c_int, [_vp, C.c_int]),
         "tlno_gpu_onee": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int]),
         "tlno_gpu_set_onee_thresholds": (C.c_int, [_vp, C.c_double, C.c_double]),
         "tlno_gpu_set_mixed_threshold": (C.c_int, [_vp, C.c_double]),
@@ -135,7 +158,11 @@ def ptr(a) -> int:
 EXPORTED = [
     "tlno_gpu_last_error", "tlno_gpu_version", "tlno_gpu_device_count", "tlno_gpu_create",
     "tlno_gpu_create_from_components", "tlno_gpu_destroy", "tlno_gpu_n_sph", "tlno_gpu_n_shells",
-    "tlno_gpu_plan", "tlno_gpu_plan_profile", "tlno_gpu_jk", "tlno_gpu_onee", "tlno_gpu_set_onee_thresholds",
+    "tlno_gpu_plan", "tlno_gpu_plan_profile", "tlno_gpu_jk", "tlno_gpu_jk_with_options", "tlno_gpu_eri_checksum",
+    "tlno_gpu_incremental_create", "tlno_gpu_incremental_destroy", "tlno_gpu_incremental_update",
+    "tlno_gpu_incremental_g", "tlno_gpu_incremental_density", "tlno_gpu_incremental_info_get",
+    "tlno_gpu_incremental_reset", "tlno_gpu_incremental_fail_next_update",
+    "tlno_gpu_onee", "tlno_gpu_set_onee_thresholds",
     "tlno_gpu_set_mixed_threshold",
     "tlno_gpu_eri_blocks", "tlno_gpu_eri_blocks_noalloc", "tlno_gpu_schwarz", "tlno_gpu_boys", "tlno_gpu_rys", "tlno_gpu_fma_peak",
     "tlno_gpu_jk_graph_capture",

@@ -31,7 +31,7 @@ def _fast_count():
 
 
 FAST_COUNT = _fast_count()
-CPP_SOURCES = ["tables.cpp", "basis.cpp", "plan.cpp", "capi.cpp"]
+CPP_SOURCES = ["tables.cpp", "basis.cpp", "plan.cpp", "capi.cpp", "incremental.cpp"]
 
 
 def _deps(src, seen=None):

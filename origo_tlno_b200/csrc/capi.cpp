@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -19,6 +20,7 @@
 #include "plan.hpp"
 #include "tables.hpp"
 #include "context.hpp"
+#include "jk_build.hpp"
 
 using namespace tlno_gpu;
 
@@ -46,6 +48,12 @@ int guarded(F&& f) {
     }
 }
 
+}  // namespace
+
+int tlno_gpu::run_guarded(const std::function<void()>& f) { return guarded(f); }
+
+namespace tlno_gpu {
+
 void set_device(int device) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -54,12 +62,6 @@ void set_device(int device) {
     }
     if (device < 0 || device >= n) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: invalid device index");
     TLNO_CUDA(cudaSetDevice(device));
-}
-
-inline bool finite_bits(double v) {
-    std::uint64_t bits;
-    std::memcpy(&bits, &v, sizeof(bits));
-    return (bits & 0x7ff0000000000000ull) != 0x7ff0000000000000ull;
 }
 
 void validate_screening(const tlno_gpu_screening& o) {
@@ -74,10 +76,20 @@ void validate_screening(const tlno_gpu_screening& o) {
         throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: density_threshold must be finite and >= 0.");
     if (!finite_bits(o.mixed_threshold) || o.mixed_threshold < 0.0)
         throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: mixed_threshold must be finite and >= 0.");
-    if (o.decay_threshold != 0.0 || o.primitive_fastschwarz_threshold != 0.0 || o.density_threshold != 0.0)
+}
+
+// Build-time combination rules of the reference's direct J/K route
+// (direct_build.ipp:104-116, then rys_engine.ipp:18253-18262 for the
+// specialised route whose single shell-level metric this engine follows).
+void validate_build_combination(const tlno_gpu_screening& o) {
+    if (o.density_threshold > 0.0 && o.decay_threshold > 0.0)
         throw Error(TLNO_GPU_E_INVALID,
-                    "tlno_gpu: decay, primitive FASTSCHWARZ and density screening are not implemented; "
-                    "set them to 0");
+                    "eri_ao_tensor_hgp: density screening requires Schwarz bounds and cannot be combined with "
+                    "the heuristic decay metric.");
+    if (o.integral_threshold != 0.0 && o.decay_threshold != 0.0)
+        throw Error(TLNO_GPU_E_INVALID,
+                    "eri_ao_tensor_hgp: pure-spherical Schwarz+decay screening is not part of the independent "
+                    "decay checkpoint; select exactly one shell-level metric.");
 }
 
 // Host-side density contract (direct_build.ipp:25-96).
@@ -98,14 +110,44 @@ void validate_density_host(const double* D, int M) {
 
 
 
-// Enqueues one J/K build on stream s over device buffers.
-void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const double* dD, double* dJ,
-                double* dK, long long total, int M_single, bool want_j, bool want_k, bool mixed,
-                double* d_dmax, float* dD32, cudaStream_t s) {
+BuildSpec spec_from(const tlno_gpu_screening& o, bool want_j, bool want_k, bool mixed, bool fused_g) {
+    BuildSpec b;
+    b.want_j = want_j;
+    b.want_k = want_k;
+    b.mixed = mixed;
+    b.mixed_threshold = o.mixed_threshold;
+    b.den_thr = o.density_threshold;
+    b.den_mode = o.density_threshold > 0.0 ? (fused_g ? 2 : 1) : 0;
+    b.fs_thr2 = o.primitive_fastschwarz_threshold * o.primitive_fastschwarz_threshold;
+    return b;
+}
+
+// Enqueues one J/K build on stream s over device buffers (the density tables
+// of a density-screened build must be allocated before: ensure_density_tables).
+void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const double* dD, double* dJ,
+                double* dK, long long total, int M_single, double* d_dmax, float* dD32, cudaStream_t s) {
+    const bool want_j = spec.want_j, want_k = spec.want_k, mixed = spec.mixed;
     TLNO_CUDA(cudaMemsetAsync(dJ, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(dK, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(plan.d_counters.ptr, 0, sizeof(int) * 2 * plan.combos.size(), s));
     if (mixed) launch_absmax_f32(dD, total, d_dmax, dD32, s);
+    dev::DensityScreen den{};
+    if (spec.den_mode) {
+        if (!plan.d_rho_blk.ptr || !plan.d_rho_max.ptr)
+            throw Error(TLNO_GPU_E_STATE, "tlno_gpu: density-screen tables not allocated");
+        const bool multi = plan.n_mol > 1;
+        launch_density_blocks(dD, multi ? plan.d_mol_mat_off.as<long long>() : nullptr,
+                              multi ? plan.d_mol_M.as<int>() : nullptr, M_single, plan.d_shell_sph.as<int>(),
+                              plan.d_shell_L.as<int>(), multi ? plan.d_mol_shell_off.as<int>() : nullptr,
+                              multi ? plan.d_mol_ns.as<int>() : nullptr, plan.mol_ns.empty() ? 0 : plan.mol_ns[0],
+                              plan.n_mol, plan.max_ns2, multi ? plan.d_rho_off.as<long long>() : nullptr,
+                              plan.d_rho_blk.as<double>(), plan.d_rho_max.as<double>(), s);
+        den.mode = spec.den_mode;
+        den.thr = spec.den_thr;
+        den.rho_blk = plan.d_rho_blk.as<double>();
+        den.rho_off = multi ? plan.d_rho_off.as<long long>() : nullptr;
+        den.rho_max = plan.d_rho_max.as<double>();
+    }
     const dev::PlanView pv = plan.view();
     int sms = 0, devid = 0;
     TLNO_CUDA(cudaGetDevice(&devid));
@@ -124,7 +166,10 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
         cl.tile_begin = 0;
         cl.tile_end = cs.n_tiles;
         cl.tau = plan.tau;
-        cl.tau_mix = mixed_threshold;
+        cl.tau_mix = spec.mixed_threshold;
+        cl.den = den;
+        cl.fs_thr2 = spec.fs_thr2;
+        cl.M_shells = plan.mol_ns.empty() ? 0 : plan.mol_ns[0];
         cl.dmax = d_dmax;
         cl.dens = dD;
         cl.dens32 = dD32;
@@ -157,7 +202,7 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, double mixed_threshold, const 
     }
 }
 
-}  // namespace
+}  // namespace tlno_gpu
 
 void tlno_gpu::set_last_error(const std::string& message) { g_error = message; }
 
@@ -166,6 +211,7 @@ namespace {
 void init_context(tlno_gpu_context* c) {
     set_device(c->device);
     ensure_device_tables();
+    noalloc_prepare(c->device);
     TLNO_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     const Basis& b = c->basis;
     const int ns = static_cast<int>(b.shells.size());
@@ -193,6 +239,32 @@ void init_context(tlno_gpu_context* c) {
     up(c->d_comp_off, b.comp_offset.data(), b.comp_offset.size() * sizeof(int));
 }
 
+// (Re)builds the context's two-electron plan for the shell-level screen of
+// `o` (Schwarz threshold or decay metric).
+void replan(tlno_gpu_context* ctx, const tlno_gpu_screening& o) {
+    TLNO_CUDA(cudaSetDevice(ctx->device));
+    if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    ctx->plan = make_plan(ctx, o);
+    ctx->screening = o;
+}
+
+}  // namespace
+
+namespace tlno_gpu {
+
+std::unique_ptr<Plan2e> make_plan(const tlno_gpu_context* ctx, const tlno_gpu_screening& o) {
+    if (ctx->basis.n_sph > 65535)
+        throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: direct J/K pair tables assume M <= 65535.");
+    auto plan = std::make_unique<Plan2e>();
+    std::vector<MolPairs> mp;
+    const double tau = o.decay_threshold > 0.0 ? o.decay_threshold : o.integral_threshold;
+    mp.push_back(build_mol_pairs(ctx->basis, o.integral_threshold, ctx->stream, o.decay_threshold));
+    build_plan(*plan, {&ctx->basis}, std::move(mp), tau, ctx->tune, ctx->stream);
+    plan->decay_metric = o.decay_threshold > 0.0;
+    return plan;
+}
+
 void ensure_work(JkWork& w, long long total) {
     const std::size_t bytes = sizeof(double) * std::max<long long>(total, 1);
     w.D.alloc(bytes);
@@ -200,6 +272,99 @@ void ensure_work(JkWork& w, long long total) {
     w.K.alloc(bytes);
     w.dmax.alloc(16);
     w.status.alloc(16);
+}
+
+}  // namespace tlno_gpu
+
+namespace {
+
+// One J/K build of a context with screening options `o` (the reference's
+// build-time ScreeningOptions): a shell-level screen other than the plan's
+// re-plans; density and primitive FASTSCHWARZ screening apply to this build.
+void run_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, double* G, int flags,
+            const tlno_gpu_screening& o) {
+    if (!ctx || !density) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
+    if (!ctx->plan) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan; call tlno_gpu_plan first");
+    const bool want_g = flags & TLNO_GPU_WANT_G;
+    const bool out_j = flags & TLNO_GPU_WANT_J, out_k = flags & TLNO_GPU_WANT_K;
+    if (!out_j && !out_k && !want_g) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: no output selected");
+    if (out_j && !J) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null J");
+    if (out_k && !K) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null K");
+    if (want_g && !G) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null G");
+    const bool dev_ptrs = flags & TLNO_GPU_DEVICE_PTRS;
+    const bool mixed = flags & TLNO_GPU_MIXED;
+    const int M = ctx->basis.n_sph;
+    const long long n = static_cast<long long>(M) * M;
+    TLNO_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    // density contract first, as the reference validates P before any option
+    // combination (direct_build.ipp:67-81)
+    const double* dD = density;
+    ensure_work(ctx->w, n);
+    if (!dev_ptrs) {
+        if (!(flags & TLNO_GPU_NO_VALIDATE)) validate_density_host(density, M);
+        TLNO_CUDA(cudaMemcpyAsync(ctx->w.D.ptr, density, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        dD = ctx->w.D.as<double>();
+    } else if (!(flags & TLNO_GPU_NO_VALIDATE)) {
+        TLNO_CUDA(cudaMemsetAsync(ctx->w.status.ptr, 0, sizeof(unsigned int), s));
+        launch_validate_density(dD, M, ctx->w.status.as<unsigned int>(), s);
+        unsigned int st = 0;
+        TLNO_CUDA(cudaMemcpyAsync(&st, ctx->w.status.ptr, sizeof(st), cudaMemcpyDeviceToHost, s));
+        TLNO_CUDA(cudaStreamSynchronize(s));
+        if (st & 1u) throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: density contains a non-finite value.");
+        if (st & 2u) throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: density must be symmetric.");
+    }
+    validate_build_combination(o);
+    if (o.integral_threshold != ctx->screening.integral_threshold ||
+        o.decay_threshold != ctx->screening.decay_threshold) {
+        const double keep_mixed = ctx->screening.mixed_threshold;
+        replan(ctx, o);
+        ctx->screening.mixed_threshold = keep_mixed;
+    }
+    const bool den = o.density_threshold > 0.0;
+    if (den) ensure_density_tables(*ctx->plan);
+    float* d32 = nullptr;
+    if (mixed) {
+        ctx->w.D32.alloc(sizeof(float) * n);
+        d32 = ctx->w.D32.as<float>();
+    }
+    tlno_gpu_screening eo = o;
+    eo.mixed_threshold = ctx->screening.mixed_threshold;
+    // Without density screening one pass serves J, K and G.  With it, J and K
+    // keep their own predicates (build_coulomb_j / build_exchange_k) and G the
+    // fused one (build_rhf_g), so G takes its own pass when J or K is also
+    // requested.
+    const bool pass_jk = out_j || out_k || !den;
+    double* dJ = (dev_ptrs && out_j) ? J : ctx->w.J.as<double>();
+    double* dK = (dev_ptrs && out_k) ? K : ctx->w.K.as<double>();
+    if (pass_jk) {
+        const bool pj = den ? out_j : (out_j || want_g);
+        const bool pk = den ? out_k : (out_k || want_g);
+        enqueue_jk(*ctx->plan, ctx->tune, spec_from(eo, pj, pk, mixed, false), dD, dJ, dK, n, M,
+                   ctx->w.dmax.as<double>(), d32, s);
+        if (!dev_ptrs) {
+            if (out_j) TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            if (out_k) TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        }
+    }
+    if (want_g) {
+        double* gJ = dJ;
+        double* gK = dK;
+        if (den) {
+            gJ = ctx->w.J.as<double>();
+            gK = ctx->w.K.as<double>();
+            enqueue_jk(*ctx->plan, ctx->tune, spec_from(eo, true, true, mixed, true), dD, gJ, gK, n, M,
+                       ctx->w.dmax.as<double>(), d32, s);
+        }
+        double* dG = G;
+        if (!dev_ptrs) {
+            ctx->w.G.alloc(sizeof(double) * std::max<long long>(n, 1));
+            dG = ctx->w.G.as<double>();
+        }
+        launch_combine_g(gJ, gK, dG, n, s);
+        if (!dev_ptrs) TLNO_CUDA(cudaMemcpyAsync(G, dG, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    }
+    TLNO_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace
@@ -262,17 +427,7 @@ int tlno_gpu_plan(tlno_gpu_context* ctx, const tlno_gpu_screening* options) {
         if (!ctx) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null context");
         tlno_gpu_screening o = options ? *options : tlno_gpu_screening{1e-12, 0, 0, 0, 1e-9};
         validate_screening(o);
-        if (ctx->basis.n_sph > 65535)
-            throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: direct J/K pair tables assume M <= 65535.");
-        TLNO_CUDA(cudaSetDevice(ctx->device));
-        ctx->screening = o;
-        if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
-        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
-        auto plan = std::make_unique<Plan2e>();
-        std::vector<MolPairs> mp;
-        mp.push_back(build_mol_pairs(ctx->basis, o.integral_threshold, ctx->stream));
-        build_plan(*plan, {&ctx->basis}, std::move(mp), o.integral_threshold, ctx->tune, ctx->stream);
-        ctx->plan = std::move(plan);
+        replan(ctx, o);
     });
 }
 
@@ -294,59 +449,72 @@ int tlno_gpu_plan_profile(const tlno_gpu_context* ctx, tlno_gpu_profile* out) {
 
 int tlno_gpu_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, double* G, int flags) {
     return guarded([&] {
-        if (!ctx || !density) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
+        if (!ctx) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
+        run_jk(ctx, density, J, K, G, flags, ctx->screening);
+    });
+}
+
+int tlno_gpu_jk_with_options(tlno_gpu_context* ctx, const double* density, double* J, double* K, double* G,
+                             int flags, const tlno_gpu_screening* options) {
+    return guarded([&] {
+        if (!ctx || !options) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
+        validate_screening(*options);
+        run_jk(ctx, density, J, K, G, flags, *options);
+    });
+}
+
+int tlno_gpu_eri_checksum(tlno_gpu_context* ctx, double* checksum, double* ms) {
+    return guarded([&] {
+        if (!ctx || !checksum) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
         if (!ctx->plan) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan; call tlno_gpu_plan first");
-        const bool want_g = flags & TLNO_GPU_WANT_G;
-        const bool want_j = (flags & TLNO_GPU_WANT_J) || want_g;
-        const bool want_k = (flags & TLNO_GPU_WANT_K) || want_g;
-        if (!want_j && !want_k) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: no output selected");
-        if ((flags & TLNO_GPU_WANT_J) && !J) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null J");
-        if ((flags & TLNO_GPU_WANT_K) && !K) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null K");
-        if (want_g && !G) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null G");
-        const bool dev_ptrs = flags & TLNO_GPU_DEVICE_PTRS;
-        const bool mixed = flags & TLNO_GPU_MIXED;
-        const int M = ctx->basis.n_sph;
-        const long long n = static_cast<long long>(M) * M;
         TLNO_CUDA(cudaSetDevice(ctx->device));
         cudaStream_t s = ctx->stream;
-        ensure_work(ctx->w, n);
-        const double* dD = density;
-        if (!dev_ptrs) {
-            if (!(flags & TLNO_GPU_NO_VALIDATE)) validate_density_host(density, M);
-            TLNO_CUDA(cudaMemcpyAsync(ctx->w.D.ptr, density, sizeof(double) * n, cudaMemcpyHostToDevice, s));
-            dD = ctx->w.D.as<double>();
-        } else if (!(flags & TLNO_GPU_NO_VALIDATE)) {
-            TLNO_CUDA(cudaMemsetAsync(ctx->w.status.ptr, 0, sizeof(unsigned int), s));
-            launch_validate_density(dD, M, ctx->w.status.as<unsigned int>(), s);
-            unsigned int st = 0;
-            TLNO_CUDA(cudaMemcpyAsync(&st, ctx->w.status.ptr, sizeof(st), cudaMemcpyDeviceToHost, s));
-            TLNO_CUDA(cudaStreamSynchronize(s));
-            if (st & 1u) throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: density contains a non-finite value.");
-            if (st & 2u) throw Error(TLNO_GPU_E_INVALID, "eri_ao_tensor_hgp: density must be symmetric.");
+        Plan2e& plan = *ctx->plan;
+        ensure_work(ctx->w, 1);
+        double* d_sum = ctx->w.dmax.as<double>();
+        int sms = 0;
+        TLNO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        const dev::PlanView pv = plan.view();
+        cudaEvent_t e0, e1;
+        TLNO_CUDA(cudaEventCreate(&e0));
+        TLNO_CUDA(cudaEventCreate(&e1));
+        TLNO_CUDA(cudaMemsetAsync(d_sum, 0, sizeof(double), s));
+        TLNO_CUDA(cudaMemsetAsync(plan.d_counters.ptr, 0, sizeof(int) * 2 * plan.combos.size(), s));
+        TLNO_CUDA(cudaEventRecord(e0, s));
+        for (std::size_t ci = 0; ci < plan.combos.size(); ++ci) {
+            ComboSchedule& cs = plan.combos[ci];
+            dev::ClassLaunch cl{};
+            cl.la = cs.la; cl.lb = cs.lb; cl.lc = cs.lc; cl.ld = cs.ld;
+            cl.same = (cs.X == cs.Y);
+            cl.bb = cs.bb;
+            cl.bk = cs.bk;
+            cl.blocks = cs.d_blocks.as<dev::BlockDesc>();
+            cl.bra_list = cs.d_bra_list.as<int>();
+            cl.tile_prefix = cs.d_prefix.as<int>();
+            cl.n_blocks = static_cast<int>(cs.blocks.size());
+            cl.tile_begin = 0;
+            cl.tile_end = cs.n_tiles;
+            cl.tau = plan.tau;
+            cl.dmax = d_sum;
+            cl.M = ctx->basis.n_sph;
+            cl.want_j = 0;
+            cl.want_k = 0;
+            cl.checksum = d_sum;
+            cl.counter = plan.d_counters.as<int>() + 2 * ci;
+            const int grid = sms * ctx->tune.grid_mult;
+            if (cs.fast)
+                launch_eri_jk_fast(pv, cl, false, grid, s);
+            else
+                launch_eri_jk_generic(pv, cl, false, ctx->tune.generic_warps, grid, s);
         }
-        double* dJ = (dev_ptrs && J && (flags & TLNO_GPU_WANT_J)) ? J : ctx->w.J.as<double>();
-        double* dK = (dev_ptrs && K && (flags & TLNO_GPU_WANT_K)) ? K : ctx->w.K.as<double>();
-        float* d32 = nullptr;
-        if (mixed) {
-            ctx->w.D32.alloc(sizeof(float) * n);
-            d32 = ctx->w.D32.as<float>();
-        }
-        enqueue_jk(*ctx->plan, ctx->tune, ctx->screening.mixed_threshold, dD, dJ, dK, n, M, want_j, want_k,
-                   mixed, ctx->w.dmax.as<double>(), d32, s);
-        if (want_g) {
-            double* dG = G;
-            if (!dev_ptrs) {
-                ctx->w.G.alloc(sizeof(double) * std::max<long long>(n, 1));
-                dG = ctx->w.G.as<double>();
-            }
-            launch_combine_g(dJ, dK, dG, n, s);
-            if (!dev_ptrs) TLNO_CUDA(cudaMemcpyAsync(G, dG, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-        }
-        if (!dev_ptrs) {
-            if (flags & TLNO_GPU_WANT_J) TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-            if (flags & TLNO_GPU_WANT_K) TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-        }
+        TLNO_CUDA(cudaEventRecord(e1, s));
+        TLNO_CUDA(cudaMemcpyAsync(checksum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, s));
         TLNO_CUDA(cudaStreamSynchronize(s));
+        float t = 0.f;
+        TLNO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (ms) *ms = t;
     });
 }
 
@@ -605,10 +773,14 @@ int tlno_gpu_jk_graph_capture(tlno_gpu_context* ctx, const double* d_density, do
             ctx->w.D32.alloc(sizeof(float) * n);
             d32 = ctx->w.D32.as<float>();
         }
+        validate_build_combination(ctx->screening);
+        if (ctx->screening.density_threshold > 0.0) ensure_density_tables(*ctx->plan);
+        const BuildSpec spec = spec_from(ctx->screening, want_j, want_k, flags & TLNO_GPU_MIXED,
+                                         (flags & TLNO_GPU_WANT_G) != 0);
         TLNO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            enqueue_jk(*ctx->plan, ctx->tune, ctx->screening.mixed_threshold, d_density, d_J, d_K, n, M, want_j,
-                       want_k, flags & TLNO_GPU_MIXED, ctx->w.dmax.as<double>(), d32, ctx->stream);
+            enqueue_jk(*ctx->plan, ctx->tune, spec, d_density, d_J, d_K, n, M, ctx->w.dmax.as<double>(), d32,
+                       ctx->stream);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(ctx->stream, &g);
@@ -641,10 +813,9 @@ void* tlno_gpu_stream(tlno_gpu_context* ctx) { return ctx ? static_cast<void*>(c
 int tlno_gpu_set_tuning(tlno_gpu_context* ctx, const tlno_gpu_tuning* t) {
     return guarded([&] {
         if (!ctx || !t) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
-        if (t->fast_bb < 1 || t->fast_bb > 4 || t->generic_bk < 1 || t->generic_bk > 4096 || t->generic_warps < 0 ||
-            t->generic_warps > 8 || t->grid_mult < 1 || t->grid_mult > 64)
+        if (t->generic_bk < 1 || t->generic_bk > 4096 || t->generic_warps < 0 || t->generic_warps > 8 ||
+            t->grid_mult < 1 || t->grid_mult > 64)
             throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: tuning value out of range");
-        ctx->tune.fast_bb = t->fast_bb;
         ctx->tune.generic_bk = t->generic_bk;
         ctx->tune.generic_warps = t->generic_warps;
         ctx->tune.grid_mult = t->grid_mult;
@@ -757,10 +928,13 @@ int tlno_gpu_batch_create(int n_mol, tlno_gpu_context* const* ctxs, const tlno_g
                 throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: batch contexts must share one device");
             b->bases.push_back(ctxs[m]->basis);
         }
-        for (int m = 0; m < n_mol; ++m) mps.push_back(build_mol_pairs(b->bases[m], o.integral_threshold, b->stream));
+        for (int m = 0; m < n_mol; ++m)
+            mps.push_back(build_mol_pairs(b->bases[m], o.integral_threshold, b->stream, o.decay_threshold));
         std::vector<const Basis*> bp;
         for (auto& x : b->bases) bp.push_back(&x);
-        build_plan(b->plan, bp, std::move(mps), o.integral_threshold, b->tune, b->stream);
+        build_plan(b->plan, bp, std::move(mps), o.decay_threshold > 0.0 ? o.decay_threshold : o.integral_threshold,
+                   b->tune, b->stream);
+        b->plan.decay_metric = o.decay_threshold > 0.0;
         b->total = b->plan.mol_mat_off.back();
         *out = b.release();
     });
@@ -814,8 +988,10 @@ int tlno_gpu_batch_jk(tlno_gpu_batch* b, const double* density, double* J, doubl
             b->w.D32.alloc(sizeof(float) * b->total);
             d32 = b->w.D32.as<float>();
         }
-        enqueue_jk(b->plan, b->tune, b->screening.mixed_threshold, dD, dJ, dK, b->total, 0, true, true,
-                   flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), d32, s);
+        validate_build_combination(b->screening);
+        if (b->screening.density_threshold > 0.0) ensure_density_tables(b->plan);
+        enqueue_jk(b->plan, b->tune, spec_from(b->screening, true, true, flags & TLNO_GPU_MIXED, false), dD, dJ, dK,
+                   b->total, 0, b->w.dmax.as<double>(), d32, s);
         if (!dev_ptrs) {
             TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
             TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
@@ -836,10 +1012,13 @@ int tlno_gpu_batch_graph_capture(tlno_gpu_batch* b, const double* d_density, dou
             b->w.D32.alloc(sizeof(float) * b->total);
             d32 = b->w.D32.as<float>();
         }
+        validate_build_combination(b->screening);
+        if (b->screening.density_threshold > 0.0) ensure_density_tables(b->plan);
+        const BuildSpec spec = spec_from(b->screening, true, true, flags & TLNO_GPU_MIXED, false);
         TLNO_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            enqueue_jk(b->plan, b->tune, b->screening.mixed_threshold, d_density, d_J, d_K, b->total, 0, true, true,
-                       flags & TLNO_GPU_MIXED, b->w.dmax.as<double>(), d32, b->stream);
+            enqueue_jk(b->plan, b->tune, spec, d_density, d_J, d_K, b->total, 0, b->w.dmax.as<double>(), d32,
+                       b->stream);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(b->stream, &g);

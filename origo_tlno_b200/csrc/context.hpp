@@ -15,6 +15,9 @@
 namespace tlno_gpu {
 // Sets the calling thread's tlno_gpu_last_error() text.
 void set_last_error(const std::string& message);
+// Resolves (once per device, current device = `device`) the device address
+// of the fixed scratch of tlno_gpu_eri_blocks_noalloc.
+void noalloc_prepare(int device);
 
 struct JkWork {
     DeviceBuffer D, J, K, G, dmax, status;

@@ -26,7 +26,14 @@ struct DevTables {
     double tmax[kMaxRoots + 1];
     double h2[kMaxRoots + 1][kMaxRoots];
     double hw[kMaxRoots + 1][kMaxRoots];
+    // FP32 interval polynomials of the mixed-precision kernels (N = 1..3):
+    // interval k of width 1/4 holds 6 coefficient rows of 2N floats
+    // (lowest power of u = 4T - k - 1/2 first); staged in shared memory.
+    const float* rys32[4];
+    int rys32_nint[4];
 };
+constexpr int kRys32PerUnitDev = 4;
+constexpr int kRys32CoefDev = 6;
 
 // Cartesian triples for |a| = 0..8 in the reference order
 // (for lx = L..0: for ly = L-lx..0), flat index = offset(L) + local.
@@ -185,6 +192,44 @@ __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
         v = v * t + c[2][i];
         v = v * t + c[1][i];
         v = v * t + c[0][i];
+        if (i < N) root[i] = v; else weight[i - N] = v;
+    }
+}
+
+// FP32 roots and weights for N <= 3 from the shared-memory interval
+// polynomials (table = the staged copy of c_tabs.rys32[N]); the Hermite
+// asymptotic form above tmax(N).
+template <int N>
+__device__ __forceinline__ void rys_roots_smem32(float T, const float* __restrict__ table, float* root,
+                                                 float* weight) {
+    if (T >= float(c_tabs.tmax[N])) {
+        const float inv = 1.0f / T;
+        const float sinv = sqrtf(inv);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            root[i] = float(c_tabs.h2[N][i]) * inv;
+            weight[i] = float(c_tabs.hw[N][i]) * sinv;
+        }
+        return;
+    }
+    const float x = T * float(kRys32PerUnitDev);
+    const int k = static_cast<int>(x);
+    const float u = x - float(k) - 0.5f;
+    const float2* rec = reinterpret_cast<const float2*>(table + k * (kRys32CoefDev * 2 * N));
+    float c[kRys32CoefDev][2 * N];
+#pragma unroll
+    for (int j = 0; j < kRys32CoefDev; ++j)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const float2 v = rec[j * N + m];
+            c[j][2 * m] = v.x;
+            c[j][2 * m + 1] = v.y;
+        }
+#pragma unroll
+    for (int i = 0; i < 2 * N; ++i) {
+        float v = c[kRys32CoefDev - 1][i];
+#pragma unroll
+        for (int j = kRys32CoefDev - 2; j >= 0; --j) v = fmaf(v, u, c[j][i]);
         if (i < N) root[i] = v; else weight[i - N] = v;
     }
 }

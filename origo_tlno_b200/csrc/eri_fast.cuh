@@ -196,7 +196,7 @@ struct QuartetGeom {
 // Phase 1 + 2 for slice G (rows ia = G, G+TPQ, ...).
 template <typename R, int LA, int LB, int LC, int LD, int G>
 __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
-                                           R* __restrict__ ks) {
+                                           double fs_thr2, const float* rtab, R* __restrict__ ks) {
     using S = FastShape<LA, LB, LC, LD>;
     constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
     R acc[ROWS > 0 ? ROWS : 1][S::NCS];
@@ -217,31 +217,40 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
         const float2* pk32 = reinterpret_cast<const float2*>(pv.prim32 + ok);
         constexpr bool F32 = std::is_same<R, float>::value;
         const R ACx = R(q.A[0] - q.C[0]), ACy = R(q.A[1] - q.C[1]), ACz = R(q.A[2] - q.C[2]);
-        for (int ib = 0; ib < npb; ++ib) {
-            R p, PAx, PAy, PAz, bw, bip;
-            double bp_x = 0.0, bp_y = 0.0, bp_z = 0.0;
+        // Primitive FASTSCHWARZ: a primitive quartet whose estimate product is
+        // below the squared threshold contributes nothing (per lane; the
+        // reference drops a SIMD packet only when every lane fails).
+        const bool fs_on = fs_thr2 > 0.0;
+        // Ket primitive outer, bra primitive inner: each lane gathers its own
+        // ket record once per bra, and the bra records (the same for every
+        // lane of the warp) are broadcast loads.
+        for (int ik = 0; ik < npk; ++ik) {
+            const double fsk = fs_on ? __ldg(pv.prim_fs + ok + ik) : 0.0;
+            R qe, QCx, QCy, QCz, kw, kip;
+            double kp_x = 0.0, kp_y = 0.0, kp_z = 0.0;
             if constexpr (F32) {
-                const float2 u0 = __ldg(pb32 + 3 * ib), u1 = __ldg(pb32 + 3 * ib + 1), u2 = __ldg(pb32 + 3 * ib + 2);
-                p = u0.x; PAx = u0.y; PAy = u1.x; PAz = u1.y; bw = u2.x; bip = u2.y;
+                const float2 u0 = __ldg(pk32 + 3 * ik), u1 = __ldg(pk32 + 3 * ik + 1), u2 = __ldg(pk32 + 3 * ik + 2);
+                qe = u0.x; QCx = u0.y; QCy = u1.x; QCz = u1.y; kw = u2.x; kip = u2.y;
             } else {
-                const double2 b0v = __ldg(pb + 3 * ib), b1v = __ldg(pb + 3 * ib + 1), b2v = __ldg(pb + 3 * ib + 2);
-                bp_x = b0v.y; bp_y = b1v.x; bp_z = b1v.y;
-                p = R(b0v.x);
-                PAx = R(bp_x - q.A[0]); PAy = R(bp_y - q.A[1]); PAz = R(bp_z - q.A[2]);
-                bw = R(b2v.x); bip = R(b2v.y);
+                const double2 k0v = __ldg(pk + 3 * ik), k1v = __ldg(pk + 3 * ik + 1), k2v = __ldg(pk + 3 * ik + 2);
+                kp_x = k0v.y; kp_y = k1v.x; kp_z = k1v.y;
+                qe = R(k0v.x);
+                QCx = R(kp_x - q.C[0]); QCy = R(kp_y - q.C[1]); QCz = R(kp_z - q.C[2]);
+                kw = R(k2v.x); kip = R(k2v.y);
             }
-            for (int ik = 0; ik < npk; ++ik) {
-                R qe, QCx, QCy, QCz, kw, kip, PQx, PQy, PQz;
+            for (int ib = 0; ib < npb; ++ib) {
+                if (fs_on && !(__ldg(pv.prim_fs + ob + ib) * fsk >= fs_thr2)) continue;
+                R p, PAx, PAy, PAz, bw, bip, PQx, PQy, PQz;
                 if constexpr (F32) {
-                    const float2 u0 = __ldg(pk32 + 3 * ik), u1 = __ldg(pk32 + 3 * ik + 1), u2 = __ldg(pk32 + 3 * ik + 2);
-                    qe = u0.x; QCx = u0.y; QCy = u1.x; QCz = u1.y; kw = u2.x; kip = u2.y;
+                    const float2 u0 = __ldg(pb32 + 3 * ib), u1 = __ldg(pb32 + 3 * ib + 1), u2 = __ldg(pb32 + 3 * ib + 2);
+                    p = u0.x; PAx = u0.y; PAy = u1.x; PAz = u1.y; bw = u2.x; bip = u2.y;
                     PQx = PAx - QCx + ACx; PQy = PAy - QCy + ACy; PQz = PAz - QCz + ACz;
                 } else {
-                    const double2 k0v = __ldg(pk + 3 * ik), k1v = __ldg(pk + 3 * ik + 1), k2v = __ldg(pk + 3 * ik + 2);
-                    const double kp_x = k0v.y, kp_y = k1v.x, kp_z = k1v.y;
-                    qe = R(k0v.x);
-                    QCx = R(kp_x - q.C[0]); QCy = R(kp_y - q.C[1]); QCz = R(kp_z - q.C[2]);
-                    kw = R(k2v.x); kip = R(k2v.y);
+                    const double2 b0v = __ldg(pb + 3 * ib), b1v = __ldg(pb + 3 * ib + 1), b2v = __ldg(pb + 3 * ib + 2);
+                    const double bp_x = b0v.y, bp_y = b1v.x, bp_z = b1v.y;
+                    p = R(b0v.x);
+                    PAx = R(bp_x - q.A[0]); PAy = R(bp_y - q.A[1]); PAz = R(bp_z - q.A[2]);
+                    bw = R(b2v.x); bip = R(b2v.y);
                     PQx = R(bp_x - kp_x); PQy = R(bp_y - kp_y); PQz = R(bp_z - kp_z);
                 }
                 const R pqs = p + qe;
@@ -250,7 +259,22 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
                 const R inv = rs * rs;
                 const R Targ = p * qe * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
                 R rt[S::N], wt[S::N];
-                rys_roots_all<R, S::N>(Targ, rt, wt);
+                if constexpr (F32 && S::N <= 3) {
+                    // FP32 interval polynomials staged in shared memory
+                    rys_roots_smem32<S::N>(Targ, rtab, rt, wt);
+                } else if constexpr (F32) {
+                    // FP64 carve-out: roots and weights of N >= 4 (high-L)
+                    // quartets come from the FP64 tables even in the FP32 pass
+                    double rd[S::N], wd[S::N];
+                    rys_roots_all<double, S::N>(double(Targ), rd, wd);
+#pragma unroll
+                    for (int r = 0; r < S::N; ++r) {
+                        rt[r] = R(rd[r]);
+                        wt[r] = R(wd[r]);
+                    }
+                } else {
+                    rys_roots_all<R, S::N>(Targ, rt, wt);
+                }
                 const R pref = R(34.98683665524972497) * bw * kw * rs;
                 const R qo = qe * inv, po = p * inv;
                 const R hbp = R(0.5) * bip, hkp = R(0.5) * kip;
@@ -317,13 +341,14 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
 template <typename R, int LA, int LB, int LC, int LD, int G = 0>
 __device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, int bra, int ket, bool active,
-                                                    const QuartetGeom& q, R* ks) {
+                                                    const QuartetGeom& q, double fs_thr2, const float* rtab,
+                                                    R* ks) {
     using S = FastShape<LA, LB, LC, LD>;
     if constexpr (G < S::TPQ) {
         if (g == G)
-            fast_slice<R, LA, LB, LC, LD, G>(pv, bra, ket, active, q, ks);
+            fast_slice<R, LA, LB, LC, LD, G>(pv, bra, ket, active, q, fs_thr2, rtab, ks);
         else
-            fast_slice_dispatch<R, LA, LB, LC, LD, G + 1>(g, pv, bra, ket, active, q, ks);
+            fast_slice_dispatch<R, LA, LB, LC, LD, G + 1>(g, pv, bra, ket, active, q, fs_thr2, rtab, ks);
     }
 }
 
@@ -359,8 +384,20 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         ks = reinterpret_cast<R*>(fast_smem) + (grp * 32 + lane) * S::LANE_STRIDE;
     const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
     const int bar_id = 1 + grp, bar_n = 32 * S::TPQ;
+    // FP32 kernels with N <= 3 stage their Rys interval polynomials in shared
+    // memory behind the row-exchange buffer.
+    const float* rtab = nullptr;
+    if constexpr (std::is_same<R, float>::value && S::N <= 3) {
+        float* t = reinterpret_cast<float*>(fast_smem + S::SMEM_DOUBLES);
+        const int n4 = c_tabs.rys32_nint[S::N] * (kRys32CoefDev * 2 * S::N) / 4;
+        const float4* src = reinterpret_cast<const float4*>(c_tabs.rys32[S::N]);
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) reinterpret_cast<float4*>(t)[i] = __ldg(src + i);
+        __syncthreads();
+        rtab = t;
+    }
     __shared__ int s_chunk[S::BBQ];
     const int ntiles = cl.tile_end - cl.tile_begin;
+    double csum = 0.0;  // ERI checksum stream: this thread's share
 
     // Dynamic schedule: every warp group takes kTileChunk consecutive tiles
     // (one bra pair x 32 kets each) from the launch counter, so all groups
@@ -397,13 +434,16 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         // for this launch (bound, triangle, precision pass) is left before
         // the ket geometry is loaded.
         const double qket = __ldg(pv.pair_Q + ket);
+        const int mol = pv.pair_mol ? __ldg(pv.pair_mol + ket) : 0;
+        // the density screen raises the Schwarz cutoff of this build
+        const double tau_t = cl.den.mode ? density_tau_min(cl, mol) : cl.tau;
         {
             bool act = false;
             for (int ib = 0; ib < S::GB && ib < bd.nbra; ++ib) {
                 const int bra = __ldg(cl.bra_list + bd.bra0 + ib);
                 if (!lane_ok || (cl.same && bd.koff + j > bra - bd.xbeg)) continue;
                 const double qq = __ldg(pv.pair_Q + bra) * qket;
-                bool a = qq >= cl.tau;
+                bool a = qq >= tau_t;
                 if (cl.prec_mode == 1) a = a && qq >= thr;
                 if (cl.prec_mode == 2) a = a && !(qq >= thr);
                 act = act || a;
@@ -424,7 +464,6 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
             q.C[k] = __ldg(pv.shell_xyz + 3 * C + k);
             q.CD[k] = q.C[k] - __ldg(pv.shell_xyz + 3 * D + k);
         }
-        const int mol = pv.pair_mol ? __ldg(pv.pair_mol + ket) : 0;
         const int M = pv.mol_M ? __ldg(pv.mol_M + mol) : cl.M;
         const long long mbase = pv.mol_mat_off ? __ldg(pv.mol_mat_off + mol) : 0;
         const double* Dm = cl.dens + mbase;
@@ -463,12 +502,22 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         for (int ib = 0; ib < S::GB && ib < bd.nbra; ++ib) {
             const int bra = __ldg(cl.bra_list + bd.bra0 + ib);
             const int i = bra - bd.xbeg;
+            const int A = __ldg(pv.pair_A + bra), B = __ldg(pv.pair_B + bra);
             bool active = lane_ok && !(cl.same && bd.koff + j > i);
+            // density screen: Coulomb and exchange contributions kept apart
+            R jon = R(1), kon = R(1);
             if (active) {
                 const double qq = __ldg(pv.pair_Q + bra) * qket;
                 active = qq >= cl.tau;
                 if (cl.prec_mode == 1) active = active && qq >= thr;
                 if (cl.prec_mode == 2) active = active && !(qq >= thr);
+                if (active && cl.den.mode) {
+                    bool lj, lk;
+                    density_live(cl, pv, mol, A, B, C, D, qq, lj, lk);
+                    active = lj || lk;
+                    jon = lj ? R(1) : R(0);
+                    kon = lk ? R(1) : R(0);
+                }
             }
             bool any;
             if constexpr (S::TPQ > 1)
@@ -478,13 +527,12 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
             if (!any) continue;
             touched = touched || active;
 
-            const int A = __ldg(pv.pair_A + bra), B = __ldg(pv.pair_B + bra);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 q.A[k] = __ldg(pv.shell_xyz + 3 * A + k);
                 q.AB[k] = q.A[k] - __ldg(pv.shell_xyz + 3 * B + k);
             }
-            fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, ks);
+            fast_slice_dispatch<R, LA, LB, LC, LD>(g, pv, bra, ket, active, q, cl.fs_thr2, rtab, ks);
             if constexpr (S::TPQ > 1) group_sync(bar_id, bar_n);
 
             // ---- bra transfer + projection per owned ket column, digestion ----
@@ -494,7 +542,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
             if (A == B) f *= R(0.5);
             if (C == D) f *= R(0.5);
             if (bra == ket) f *= R(0.5);
-            const R fj = R(4) * f, fk = R(2) * f;
+            const R fj = R(4) * f * jon, fk = R(2) * f * kon;
             const R ABr[3] = {R(q.AB[0]), R(q.AB[1]), R(q.AB[2])};
 
             R jab[S::NSAB];
@@ -537,6 +585,13 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                                     ABr, [&](auto FU) { return ks[TLNO_CI(FU) * S::NSCD + t]; });
                             });
                         });
+                        if (cl.checksum) {
+#pragma unroll
+                            for (int e = 0; e < S::NSAB; ++e)
+                                if (canonical_element(A == B, C == D, bra == ket, a0, e / S::NSB, b0, e % S::NSB, c0,
+                                                      sc, d0, sd))
+                                    csum += double(V[e]);
+                        }
                         if (cl.want_j) {
                             R s = R(0);
 #pragma unroll
@@ -636,6 +691,11 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         }
     }
     }
+    if (cl.checksum) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) csum += __shfl_xor_sync(0xffffffffu, csum, o);
+        if (lane == 0 && csum != 0.0) atomicAdd(cl.checksum, csum);
+    }
 }
 
 // Launch geometry of class (la lb|lc ld) for the host.
@@ -645,6 +705,8 @@ template <int LA, int LB, int LC, int LD>
 constexpr int fast_bras() { return FastShape<LA, LB, LC, LD>::GB; }
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_smem_bytes() { return FastShape<LA, LB, LC, LD>::SMEM_DOUBLES * 8; }
+template <int LA, int LB, int LC, int LD>
+constexpr int fast_roots() { return FastShape<LA, LB, LC, LD>::N; }
 
 }  // namespace dev
 }  // namespace tlno_gpu

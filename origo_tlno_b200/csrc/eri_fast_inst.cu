@@ -7,6 +7,7 @@
 #include "fast_classes.hpp"
 #include "device_common.cuh"
 #include "eri_fast.cuh"
+#include "tables.hpp"
 
 #ifndef TLNO_FAST_ID
 #error "TLNO_FAST_ID must be defined"
@@ -14,38 +15,41 @@
 
 namespace tlno_gpu {
 
+// Dynamic shared memory: the row-exchange buffer of a sliced class, plus the
+// FP32 Rys interval polynomials in the FP32 kernels with N <= 3.
 #define TLNO_FAST_IMPL(id, a, b, c, d)                                                                  \
+    static int fast_smem_##id(bool fp32) {                                                              \
+        constexpr int n = dev::fast_roots<a, b, c, d>();                                                \
+        int bytes = dev::fast_smem_bytes<a, b, c, d>();                                                 \
+        if (fp32 && n <= kRys32MaxN) bytes += rys32_intervals(n) * (kRys32Deg + 1) * 2 * n * 4;         \
+        return bytes;                                                                                   \
+    }                                                                                                   \
     void fast_upload_##id(const dev::DevTables& t, const dev::CartTable& ct, const dev::C2STable& cs) {  \
         dev::upload_constant_tables(t, ct, cs);                                                         \
-        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
-        if (smem > 48 * 1024) {                                                                         \
-            cudaFuncSetAttribute(dev::eri_fast_jk_kernel<double, a, b, c, d>,                           \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);                    \
-            cudaFuncSetAttribute(dev::eri_fast_jk_kernel<float, a, b, c, d>,                            \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);                    \
-        }                                                                                               \
+        cudaFuncSetAttribute(dev::eri_fast_jk_kernel<double, a, b, c, d>,                               \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, fast_smem_##id(false));       \
+        cudaFuncSetAttribute(dev::eri_fast_jk_kernel<float, a, b, c, d>,                                \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, fast_smem_##id(true));        \
     }                                                                                                   \
     int fast_bras_##id() { return dev::fast_bras<a, b, c, d>(); }                                       \
     int fast_blocks_per_sm_##id(bool fp32) {                                                            \
         constexpr int threads = 32 * dev::fast_warps<a, b, c, d>();                                     \
-        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
         int n = 0;                                                                                      \
         if (fp32)                                                                                       \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::eri_fast_jk_kernel<float, a, b, c, d>, \
-                                                          threads, smem);                               \
+                                                          threads, fast_smem_##id(true));               \
         else                                                                                            \
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dev::eri_fast_jk_kernel<double, a, b, c, d>, \
-                                                          threads, smem);                               \
+                                                          threads, fast_smem_##id(false));              \
         return n > 0 ? n : 1;                                                                           \
     }                                                                                                   \
     void fast_launch_##id(bool fp32, const dev::PlanView& pv, const dev::ClassLaunch& cl, int grid,     \
                           cudaStream_t s) {                                                             \
         constexpr int threads = 32 * dev::fast_warps<a, b, c, d>();                                     \
-        constexpr int smem = dev::fast_smem_bytes<a, b, c, d>();                                        \
         if (fp32)                                                                                       \
-            dev::eri_fast_jk_kernel<float, a, b, c, d><<<grid, threads, smem, s>>>(pv, cl);             \
+            dev::eri_fast_jk_kernel<float, a, b, c, d><<<grid, threads, fast_smem_##id(true), s>>>(pv, cl); \
         else                                                                                            \
-            dev::eri_fast_jk_kernel<double, a, b, c, d><<<grid, threads, smem, s>>>(pv, cl);            \
+            dev::eri_fast_jk_kernel<double, a, b, c, d><<<grid, threads, fast_smem_##id(false), s>>>(pv, cl); \
     }
 
 #define TLNO_FAST_SELECT(id, a, b, c, d) \

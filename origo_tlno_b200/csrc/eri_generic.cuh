@@ -130,10 +130,13 @@ __device__ __forceinline__ void build_pair_projector(double* Pm, int la, int lb,
 
 // build_pb = false reuses the bra projector this warp built for the same
 // bra pair (it lives in its own region of the warp's shared memory).
+// jon / kon (J/K mode) are 0 when the density screen drops the quartet's
+// Coulomb / exchange contributions.
 template <typename R, int MODE>
 __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
                                 const GenericLayout& lay, double* wsm, int lane,
-                                int bra, int ket, int quartet_id, bool build_pb = true) {
+                                int bra, int ket, int quartet_id, bool build_pb = true,
+                                double jon = 1.0, double kon = 1.0) {
     const int A = pv.pair_A[bra], B = pv.pair_B[bra];
     const int C = pv.pair_A[ket], D = pv.pair_B[ket];
     const double* xa = pv.shell_xyz + 3 * A;
@@ -155,6 +158,10 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
     const int n_items = npb * npk * nroots;
     const int gslot = 3 * lay.gs;
     const int offa = cart_offset(la), offc = cart_offset(lc);
+    // Primitive FASTSCHWARZ (J/K mode, classes up to f as the reference's
+    // shell4 portfolio): a dropped primitive quartet gets a zero seed.
+    const bool fs_on = MODE == kJK && cl.fs_thr2 > 0.0 && la <= 3 && lb <= 3 && lc <= 3 && ld <= 3;
+    const int pob = pv.pair_prim_off[bra], pok = pv.pair_prim_off[ket];
     __syncwarp();
     for (int base = 0; base < n_items; base += kGenericBatch) {
         const int item = base + lane;
@@ -170,8 +177,17 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
             const R PQx = R(bp.Px) - R(kp.Px), PQy = R(bp.Py) - R(kp.Py), PQz = R(bp.Pz) - R(kp.Pz);
             const R Targ = p * q * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
             R t2, wt;
-            rys_root<R>(nroots, Targ, r, t2, wt);
-            const R pref = R(34.98683665524972497) * R(bp.w) * R(kp.w) / sqrt(pqs);
+            if (sizeof(R) == 4 && nroots >= 4) {
+                // FP64 carve-out of the FP32 pass: high-L roots and weights
+                double t2d, wtd;
+                rys_root<double>(nroots, double(Targ), r, t2d, wtd);
+                t2 = R(t2d);
+                wt = R(wtd);
+            } else {
+                rys_root<R>(nroots, Targ, r, t2, wt);
+            }
+            R pref = R(34.98683665524972497) * R(bp.w) * R(kp.w) / sqrt(pqs);
+            if (fs_on && !(pv.prim_fs[pob + ib] * pv.prim_fs[pok + ik] >= cl.fs_thr2)) pref = R(0);
             const R qo = q * inv, po = p * inv;
             const R b00 = R(0.5) * inv * t2;
             const R b10 = R(0.5) * R(bp.invp) * (R(1) - qo * t2);
@@ -244,6 +260,22 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
         // K[ad] += 2f V P[bc], K[bc] += 2f V P[ad], K[bd] += 2f V P[ac];
         // the final pass symmetrises (X + X^T)/2 (consumer_policies.ipp:87-157,
         // direct_build.ipp:471-482 for the same algebra at AO level).
+        if (cl.checksum) {
+            // ERI checksum stream: canonical unique elements of the block
+            const int a0 = pv.shell_sph[A], b0 = pv.shell_sph[B];
+            const int c0 = pv.shell_sph[C], d0 = pv.shell_sph[D];
+            double s = 0.0;
+            for (int e = lane; e < lay.nsab * lay.nscd; e += 32) {
+                const int sab = e / lay.nscd, scd = e - sab * lay.nscd;
+                if (canonical_element(A == B, C == D, bra == ket, a0, sab / lay.nb, b0, sab % lay.nb, c0,
+                                      scd / lay.nd, d0, scd % lay.nd))
+                    s += V[e];
+            }
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0 && s != 0.0) atomicAdd(cl.checksum, s);
+            __syncwarp();
+            return;
+        }
         const int mol = pv.pair_mol ? pv.pair_mol[bra] : 0;
         const int M = pv.mol_M ? pv.mol_M[mol] : cl.M;
         const long long mbase = pv.mol_mat_off ? pv.mol_mat_off[mol] : 0;
@@ -271,7 +303,7 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
         for (int e = lane; e < na * nc; e += 32) Pac[e] = Dm[(long long)(a0 + e / nc) * M + c0 + e % nc];
         __syncwarp();
         const int nscd = lay.nscd;
-        if (cl.want_j) {
+        if (cl.want_j && jon != 0.0) {
             const double fj = 4.0 * f;
             for (int sab = lane; sab < na * nb; sab += 32) {
                 double s = 0.0;
@@ -284,7 +316,7 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
                 atomicAdd(Jm + (long long)(c0 + scd / nd) * M + d0 + scd % nd, fj * s);
             }
         }
-        if (cl.want_k) {
+        if (cl.want_k && kon != 0.0) {
             const double fk = 2.0 * f;
             for (int e = lane; e < na * nc; e += 32) {
                 const int a = e / nc, c = e % nc;
@@ -359,7 +391,14 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
             if (!(qq >= cl.tau)) continue;
             if (cl.prec_mode == 1 && !(qq >= thr)) continue;
             if (cl.prec_mode == 2 && qq >= thr) continue;
-            generic_quartet<R, kJK>(pv, cl, lay, wsm, lane, bra, ket, 0, bra != pb_bra);
+            bool lj = true, lk = true;
+            if (cl.den.mode) {
+                const int mol = pv.pair_mol ? pv.pair_mol[ket] : 0;
+                density_live(cl, pv, mol, pv.pair_A[bra], pv.pair_B[bra], pv.pair_A[ket], pv.pair_B[ket], qq, lj, lk);
+                if (!lj && !lk) continue;
+            }
+            generic_quartet<R, kJK>(pv, cl, lay, wsm, lane, bra, ket, 0, bra != pb_bra, lj ? 1.0 : 0.0,
+                                    lk ? 1.0 : 0.0);
             pb_bra = bra;
         }
     }

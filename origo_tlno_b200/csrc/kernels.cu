@@ -3,6 +3,7 @@
 // host launch wrappers.
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <set>
@@ -228,6 +229,104 @@ __global__ void validate_density_kernel(const double* D, int M, unsigned int* st
     if (bits) atomicOr(status, bits);
 }
 
+// Density tables of the CVHF screen, per molecule (blockIdx.y): the ns x ns
+// table of max |D| over each shell block and its transpose (the symmetric
+// maximum the reference keeps per group pair, direct_build.ipp:122-205) and
+// rho_max[mol] = max |D| (the largest block maximum).
+__global__ void density_blocks_kernel(const double* D, const long long* mat_off, const int* mol_M, int M1,
+                                      const int* shell_sph, const int* shell_L, const int* mol_shell_off,
+                                      const int* mol_ns, int ns1, const long long* blk_off, double* blk,
+                                      double* rho_max) {
+    __shared__ double red[32];
+    const int mol = blockIdx.y;
+    const int M = mol_M ? mol_M[mol] : M1;
+    const int ns = mol_ns ? mol_ns[mol] : ns1;
+    const int so = mol_shell_off ? mol_shell_off[mol] : 0;
+    const double* Dm = D + (mat_off ? mat_off[mol] : 0);
+    double* out = blk + (blk_off ? blk_off[mol] : 0);
+    const long long n = (long long)ns * ns;
+    double m = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int i = static_cast<int>(e / ns), j = static_cast<int>(e % ns);
+        const int r0 = shell_sph[so + i], c0 = shell_sph[so + j];
+        const int nr = 2 * shell_L[so + i] + 1, nc = 2 * shell_L[so + j] + 1;
+        double v = 0.0;
+        for (int r = 0; r < nr; ++r)
+            for (int c = 0; c < nc; ++c) {
+                v = fmax(v, fabs(Dm[(long long)(r0 + r) * M + c0 + c]));
+                v = fmax(v, fabs(Dm[(long long)(c0 + c) * M + r0 + r]));
+            }
+        out[e] = v;
+        m = fmax(m, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0)
+            atomicMax(reinterpret_cast<unsigned long long*>(rho_max + mol),
+                      static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// Incremental-state density step: delta = Dn - Dp (Dp null: first density,
+// delta unused), status bit 1 = Dn non-finite, bit 2 = delta non-finite,
+// bit 4 = some delta element nonzero; *dmax = max |delta| (max |Dn| without
+// Dp), zeroed by the launcher.
+__global__ void density_delta_kernel(const double* Dn, const double* Dp, double* delta, long long n,
+                                     unsigned int* status, double* dmax) {
+    __shared__ double red[32];
+    unsigned int bits = 0;
+    double m = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double v = Dn[e];
+        if ((__double_as_longlong(v) & 0x7ff0000000000000ll) == 0x7ff0000000000000ll) {
+            bits |= 1u;
+            continue;
+        }
+        double d = v;
+        if (Dp) {
+            d = v - Dp[e];
+            delta[e] = d;
+            if ((__double_as_longlong(d) & 0x7ff0000000000000ll) == 0x7ff0000000000000ll) {
+                bits |= 2u;
+                continue;
+            }
+            if (d != 0.0) bits |= 4u;
+        }
+        m = fmax(m, fabs(d));
+    }
+    if (bits) atomicOr(status, bits);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0)
+            atomicMax(reinterpret_cast<unsigned long long*>(dmax), static_cast<unsigned long long>(__double_as_longlong(m)));
+    }
+}
+
+// out = Gp + dG (Gp null: out = dG); status bit 1 = dG non-finite, bit 2 =
+// out non-finite.
+__global__ void g_accumulate_kernel(const double* Gp, const double* dG, double* out, long long n, unsigned int* status) {
+    unsigned int bits = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double d = dG[e];
+        if ((__double_as_longlong(d) & 0x7ff0000000000000ll) == 0x7ff0000000000000ll) {
+            bits |= 1u;
+            continue;
+        }
+        const double v = Gp ? Gp[e] + d : d;
+        if ((__double_as_longlong(v) & 0x7ff0000000000000ll) == 0x7ff0000000000000ll) bits |= 2u;
+        out[e] = v;
+    }
+    if (bits) atomicOr(status, bits);
+}
+
 __global__ void combine_g_kernel(const double* J, const double* K, double* G, long long n) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
         G[e] = J[e] - 0.5 * K[e];
@@ -306,6 +405,10 @@ void ensure_device_tables() {
             t.h2[n][i] = h.herm_root2[n][i];
             t.hw[n][i] = h.herm_weight[n][i];
         }
+    }
+    for (int n = 1; n <= kRys32MaxN; ++n) {
+        t.rys32[n] = upload(rys32_table(n));
+        t.rys32_nint[n] = rys32_intervals(n);
     }
     CartTable ct{};
     build_cart(ct);
@@ -458,6 +561,37 @@ void launch_validate_density(const double* D, int M, unsigned int* status, cudaS
     const long long n = (long long)M * M;
     const int grid = static_cast<int>(std::min<long long>((n + 255) / 256, sm_count() * 16));
     validate_density_kernel<<<std::max(grid, 1), 256, 0, s>>>(D, M, status);
+    TLNO_CUDA(cudaGetLastError());
+}
+
+void launch_density_blocks(const double* D, const long long* mat_off, const int* mol_M, int M1, const int* shell_sph,
+                           const int* shell_L, const int* mol_shell_off, const int* mol_ns, int ns1, int n_mol,
+                           long long max_entries, const long long* blk_off, double* blk, double* rho_max,
+                           cudaStream_t s) {
+    if (n_mol <= 0) return;
+    TLNO_CUDA(cudaMemsetAsync(rho_max, 0, sizeof(double) * n_mol, s));
+    const int gx = static_cast<int>(std::max<long long>(1, std::min<long long>((max_entries + 255) / 256,
+                                                                                sm_count() * 8)));
+    dim3 grid(gx, n_mol);
+    density_blocks_kernel<<<grid, 256, 0, s>>>(D, mat_off, mol_M, M1, shell_sph, shell_L, mol_shell_off, mol_ns, ns1,
+                                               blk_off, blk, rho_max);
+    TLNO_CUDA(cudaGetLastError());
+}
+
+void launch_density_delta(const double* Dn, const double* Dp, double* delta, long long n, unsigned int* status,
+                          double* dmax, cudaStream_t s) {
+    TLNO_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned int), s));
+    TLNO_CUDA(cudaMemsetAsync(dmax, 0, sizeof(double), s));
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, sm_count() * 8)));
+    density_delta_kernel<<<grid, 256, 0, s>>>(Dn, Dp, delta, n, status, dmax);
+    TLNO_CUDA(cudaGetLastError());
+}
+
+void launch_g_accumulate(const double* Gp, const double* dG, double* out, long long n, unsigned int* status,
+                         cudaStream_t s) {
+    TLNO_CUDA(cudaMemsetAsync(status, 0, sizeof(unsigned int), s));
+    const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>((n + 255) / 256, sm_count() * 8)));
+    g_accumulate_kernel<<<grid, 256, 0, s>>>(Gp, dG, out, n, status);
     TLNO_CUDA(cudaGetLastError());
 }
 

@@ -43,6 +43,22 @@ void launch_absmax_f32(const double* x, long long n, double* out, float* x32, cu
 // Density contract check: bit 1 = non-finite entry, bit 2 = asymmetric
 // beyond 128 eps * max(1, |Dij|, |Dji|) (direct_build.ipp:25-96).
 void launch_validate_density(const double* D, int M, unsigned int* status, cudaStream_t s);
+// CVHF density tables per molecule: blk[off[mol] + i * ns + j] = max |D| over
+// shell block (i, j) and its transpose, rho_max[mol] = max |D| (zeroed here).
+// Single molecule: null per-molecule arrays, M1 / ns1 give the sizes.
+void launch_density_blocks(const double* D, const long long* mat_off, const int* mol_M, int M1, const int* shell_sph,
+                           const int* shell_L, const int* mol_shell_off, const int* mol_ns, int ns1, int n_mol,
+                           long long max_entries, const long long* blk_off, double* blk, double* rho_max,
+                           cudaStream_t s);
+// delta = Dn - Dp with the incremental state's checks: status bit 1 = Dn
+// non-finite, 2 = delta non-finite, 4 = delta nonzero somewhere; *dmax =
+// max |delta| (max |Dn| when Dp is null; delta then untouched).
+void launch_density_delta(const double* Dn, const double* Dp, double* delta, long long n, unsigned int* status,
+                          double* dmax, cudaStream_t s);
+// out = Gp + dG (or dG when Gp is null); status bit 1 = dG non-finite,
+// 2 = out non-finite.
+void launch_g_accumulate(const double* Gp, const double* dG, double* out, long long n, unsigned int* status,
+                         cudaStream_t s);
 // G = J - K / 2 over n elements.
 void launch_combine_g(const double* J, const double* K, double* G, long long n, cudaStream_t s);
 // Dependent-chain FMA throughput probe: returns TFLOP/s.

@@ -32,6 +32,28 @@ struct PlanView {
     // Per-molecule matrix bases (batch): density/J/K at base + M*M offsets.
     const long long* mol_mat_off; // element offset of the molecule's M x M block
     const int* mol_M;
+    // Primitive FASTSCHWARZ estimate per primitive pair (same order as prim):
+    // 24.7394... w^2 sqrt(1/p) (rys_engine.ipp:2264-2268); may be null.
+    const double* prim_fs;
+    // Per molecule: first global shell and shell count (density tables are
+    // indexed by molecule-local shells); null for a single molecule.
+    const int* mol_shell_off;
+    const int* mol_ns;
+};
+
+// Density (CVHF) screen of one build (direct_build.ipp:122-251,
+// native_quartets.ipp:499-518): a quartet of pair metric product q passes the
+// Coulomb test when q >= max(tau, thr / (4 rho_max)) and
+// q * 4 max(rho_ab, rho_cd) >= thr, the exchange test when
+// q >= max(tau, thr / rho_max) and q * max(rho_ac, rho_ad, rho_bc, rho_bd) >= thr,
+// the fused (G) test when q >= max(tau, thr / (4 rho_max)) and
+// q * max(coulomb cap, exchange cap) >= thr.
+struct DensityScreen {
+    int mode;                     // 0 off; 1 J and K tested apart; 2 fused G test
+    double thr;                   // density_threshold
+    const double* rho_blk;        // per molecule ns x ns shell-block maxima of |D| (flat)
+    const long long* rho_off;     // per molecule offset into rho_blk (null: single molecule)
+    const double* rho_max;        // per molecule max |D|
 };
 
 // One block of a quartet-class schedule: `nbra` bra pairs (entries bra0 ..
@@ -77,8 +99,14 @@ struct ClassLaunch {
     double* J;
     double* K;
     int M;                        // single-molecule AO count (when no batch)
+    int M_shells;                 // single-molecule shell count (when no batch)
     int want_j, want_k;
     unsigned int* status;         // device error word (0 = ok)
+    DensityScreen den;
+    double fs_thr2;               // primitive FASTSCHWARZ threshold squared (0 = off)
+    // ERI checksum stream (J/K kernels with want_j = want_k = 0): the sum of
+    // the canonical unique spherical ERIs of the launch is added here.
+    double* checksum;
 };
 
 struct OneePair {

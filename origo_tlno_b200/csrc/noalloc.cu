@@ -7,11 +7,13 @@
 //
 // The per-call scratch of the ERI-block kernel (the ad-hoc shell-pair table,
 // the primitive-pair records and the class-sorted quartet lists) lives in
-// one file-scope device array of kNoAllocScratchBytes.  Every device that
-// loads this library holds that array until process exit.  Its device address
-// is looked up once per device (cudaGetSymbolAddress, with that device
-// current) by the first call on that device; that first call should
-// therefore come before any stream capture.  All calls share the one array,
+// one file-scope device array of kNoAllocScratchBytes.  Every device on which
+// a context is created holds that array until process exit: context creation
+// looks up its device address (cudaGetSymbolAddress, with that device
+// current), which also loads this file's device code under lazy module
+// loading, so the 8 MiB are taken then and never by the entry point itself.
+// A call on a device without a context looks the address up itself and
+// should therefore come before any stream capture.  All calls share the one array,
 // so calls whose work overlaps on the GPU (for instance two contexts driven
 // from two host threads) race on it.  A call rewrites every scratch byte it
 // reads before the kernels read it, so nothing left by an earlier call has to
@@ -54,6 +56,8 @@ void* scratch_address(int device) {
 std::size_t align256(std::size_t n) { return (n + 255) & ~static_cast<std::size_t>(255); }
 
 }  // namespace
+
+void tlno_gpu::noalloc_prepare(int device) { (void)scratch_address(device); }
 
 extern "C" int tlno_gpu_eri_blocks_noalloc(tlno_gpu_context* ctx, int n_quartets, const int* shells4,
                                            const long long* offsets, double* d_out) {

@@ -24,6 +24,10 @@
 namespace tlno_gpu {
 
 namespace {
+// Simint's binary64 FASTSCHWARZ prefactor sqrt(2) pi^{5/2} (the literal the
+// reference keeps, rys_engine.ipp:68-72).
+constexpr double kFastSchwarzPrefactor = 24.739429451193148050228357586821944304008810699990039583;
+
 // Schwarz bucket of a pair: floor(-log2 Q), so bucket k holds
 // Q in (2^-(k+1), 2^-k]; larger Q first.
 int Q_bucket(double q) {
@@ -124,12 +128,47 @@ void primitive_pairs(const Basis& b, int A, int B, std::vector<dev::DPrimPair>& 
     }
 }
 
-MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s) {
+// Decay scale of a shell (alpha_min, K = sum_i |c_i| (pi / alpha_i)^{3/4})
+// and the pair indicator K_A K_B exp(-mu |AB|^2), mu from the two smallest
+// exponents (rys_engine.ipp:2205-2241).
+namespace {
+struct DecayScale {
+    double alpha_min = 0.0, K = 0.0;
+};
+DecayScale decay_scale(const Basis& b, int sh) {
+    const Shell& s = b.shells[sh];
+    DecayScale out;
+    if (s.nprim == 0) return out;
+    out.alpha_min = b.exps[s.prim_offset];
+    for (int i = 0; i < s.nprim; ++i) {
+        const double alpha = b.exps[s.prim_offset + i];
+        out.alpha_min = std::min(out.alpha_min, alpha);
+        out.K += std::fabs(b.c_radial[s.prim_offset + i]) * std::pow(kPi / alpha, 0.75);
+    }
+    return out;
+}
+double pair_decay_bound(const Basis& b, int A, int B, const DecayScale& a, const DecayScale& c) {
+    if (!(a.alpha_min > 0.0) || !(c.alpha_min > 0.0)) return 0.0;
+    const double dx = b.shells[A].center[0] - b.shells[B].center[0];
+    const double dy = b.shells[A].center[1] - b.shells[B].center[1];
+    const double dz = b.shells[A].center[2] - b.shells[B].center[2];
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const double mu = a.alpha_min * c.alpha_min / (a.alpha_min + c.alpha_min);
+    return a.K * c.K * std::exp(-mu * r2);
+}
+}  // namespace
+
+MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s, double decay) {
     MolPairs mp;
     const int ns = static_cast<int>(b.shells.size());
     const long long npairs = static_cast<long long>(ns) * (ns + 1) / 2;
     mp.Q_canonical.assign(static_cast<std::size_t>(npairs), 0.0);
     if (ns == 0) return mp;
+    const bool use_decay = decay > 0.0;
+    if (use_decay) tau = decay;
+    std::vector<DecayScale> dscale;
+    if (use_decay)
+        for (int i = 0; i < ns; ++i) dscale.push_back(decay_scale(b, i));
 
     // Device copy of the shells for the Schwarz kernel.
     std::vector<double> xyz(3 * ns);
@@ -200,7 +239,7 @@ MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s) {
             list.insert(list.end(), by_cls[c].begin(), by_cls[c].end());
         }
         upload_vec(d_list, list, s);
-        for (int c = 0; c < kMaxPairClasses; ++c) {
+        for (int c = 0; c < kMaxPairClasses && !use_decay; ++c) {
             const int cnt = list_off[c + 1] - list_off[c];
             if (cnt == 0) continue;
             int la = 0;
@@ -214,10 +253,14 @@ MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s) {
             cl.out = d_Q.as<double>() + list_off[c];
             launch_eri_schwarz(pv, cl, s);
         }
-        std::vector<double> qsorted(n);
-        TLNO_CUDA(cudaMemcpyAsync(qsorted.data(), d_Q.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
-        TLNO_CUDA(cudaStreamSynchronize(s));
-        for (int pos = 0; pos < n; ++pos) mp.Q_canonical[c0 + list[pos]] = qsorted[pos];
+        if (use_decay) {
+            for (int t = 0; t < n; ++t) mp.Q_canonical[c0 + t] = pair_decay_bound(b, A[t], B[t], dscale[A[t]], dscale[B[t]]);
+        } else {
+            std::vector<double> qsorted(n);
+            TLNO_CUDA(cudaMemcpyAsync(qsorted.data(), d_Q.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+            TLNO_CUDA(cudaStreamSynchronize(s));
+            for (int pos = 0; pos < n; ++pos) mp.Q_canonical[c0 + list[pos]] = qsorted[pos];
+        }
         // remember pair metadata in canonical order for the selection below
         for (int t = 0; t < n; ++t) {
             mp.A.push_back(A[t]);
@@ -287,6 +330,9 @@ dev::PlanView Plan2e::view() const {
     pv.prim32 = d_prim32.as<dev::FPrimPair>();
     pv.mol_mat_off = n_mol > 1 ? d_mol_mat_off.as<long long>() : nullptr;
     pv.mol_M = n_mol > 1 ? d_mol_M.as<int>() : nullptr;
+    pv.prim_fs = d_prim_fs.as<double>();
+    pv.mol_shell_off = n_mol > 1 ? d_mol_shell_off.as<int>() : nullptr;
+    pv.mol_ns = n_mol > 1 ? d_mol_ns.as<int>() : nullptr;
     return pv;
 }
 
@@ -338,6 +384,7 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
     plan.kept_pairs = static_cast<long long>(plan.pair_A.size());
     std::vector<dev::DPrimPair> prim(static_cast<std::size_t>(prim_total));
     std::vector<dev::FPrimPair> prim32(static_cast<std::size_t>(prim_total));
+    std::vector<double> prim_fs(static_cast<std::size_t>(prim_total));
     {
         const long long np = static_cast<long long>(plan.pair_A.size());
         parallel_for(np, [&](long long b0, long long e0) {
@@ -351,6 +398,10 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
                 const auto& ca = bases[m]->shells[plan.pair_A[k] - so].center;
                 for (std::size_t t = 0; t < tmp.size(); ++t) {
                     const dev::DPrimPair& d = tmp[t];
+                    // Simint's FASTSCHWARZ primitive-pair value, squared MEST
+                    // estimate sqrt(2) pi^{5/2} p^{-5/2} e^{-2 mu R^2} (cA cB)^2
+                    // (rys_engine.ipp:68-72, 2264-2268)
+                    prim_fs[plan.pair_prim_off[k] + t] = kFastSchwarzPrefactor * d.w * d.w * std::sqrt(d.invp);
                     prim32[plan.pair_prim_off[k] + t] = {static_cast<float>(d.p), static_cast<float>(d.Px - ca[0]),
                                                          static_cast<float>(d.Py - ca[1]), static_cast<float>(d.Pz - ca[2]),
                                                          static_cast<float>(d.w), static_cast<float>(d.invp)};
@@ -371,6 +422,19 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
     upload_vec(plan.d_prim32, prim32, s);
     upload_vec(plan.d_mol_mat_off, plan.mol_mat_off, s);
     upload_vec(plan.d_mol_M, plan.mol_M, s);
+    upload_vec(plan.d_prim_fs, prim_fs, s);
+    plan.mol_ns.assign(plan.n_mol, 0);
+    plan.rho_off.assign(plan.n_mol + 1, 0);
+    plan.max_ns2 = 0;
+    for (int m = 0; m < plan.n_mol; ++m) {
+        plan.mol_ns[m] = plan.mol_shell_off[m + 1] - plan.mol_shell_off[m];
+        const long long n2 = static_cast<long long>(plan.mol_ns[m]) * plan.mol_ns[m];
+        plan.rho_off[m + 1] = plan.rho_off[m] + n2;
+        plan.max_ns2 = std::max(plan.max_ns2, n2);
+    }
+    upload_vec(plan.d_mol_shell_off, plan.mol_shell_off, s);
+    upload_vec(plan.d_mol_ns, plan.mol_ns, s);
+    upload_vec(plan.d_rho_off, plan.rho_off, s);
 
     // Quartet-class schedules.
     plan.combos.clear();
@@ -541,6 +605,11 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
     }
     plan.d_counters.alloc(sizeof(int) * 2 * std::max<std::size_t>(plan.combos.size(), 1));
     TLNO_CUDA(cudaStreamSynchronize(s));
+}
+
+void ensure_density_tables(Plan2e& plan) {
+    plan.d_rho_blk.alloc(sizeof(double) * std::max<long long>(plan.rho_off.empty() ? 1 : plan.rho_off.back(), 1));
+    plan.d_rho_max.alloc(sizeof(double) * std::max(plan.n_mol, 1));
 }
 
 void build_onee_plan(OneePlan& p, const Basis& b, double decay_eps, double nuclear_eps) {

@@ -12,7 +12,6 @@
 namespace tlno_gpu {
 
 struct Tuning {
-    int fast_bb = 4;        // accepted and ignored (compile-time kernels take one bra per tile)
     int generic_bk = 64;    // ket pairs per tile of the warp-per-quartet kernel
     int generic_warps = 0;  // 0 = from shared-memory budget
     int grid_mult = 8;      // CTAs per SM for persistent launches
@@ -60,6 +59,18 @@ public:
     DeviceBuffer d_shell_xyz, d_shell_L, d_shell_sph;
     DeviceBuffer d_pair_A, d_pair_B, d_pair_prim_off, d_pair_nprim, d_pair_Q, d_pair_mol;
     DeviceBuffer d_prim, d_prim32, d_mol_mat_off, d_mol_M;
+    // Primitive FASTSCHWARZ estimate per primitive pair (prim order).
+    DeviceBuffer d_prim_fs;
+    // Density-screen tables: per molecule shell offset and count, offsets of
+    // the ns x ns block tables, the tables and max |D| (allocated on first
+    // use of density screening).
+    std::vector<int> mol_ns;
+    std::vector<long long> rho_off;
+    DeviceBuffer d_mol_shell_off, d_mol_ns, d_rho_off, d_rho_blk, d_rho_max;
+    long long max_ns2 = 0;
+    // Shell-level metric of this plan: false = Schwarz bounds, true = the
+    // heuristic decay indicator (integral_threshold must then be 0).
+    bool decay_metric = false;
     long long total_quartets = 0, total_prim_quartets = 0;
     double total_flops = 0.0;
     long long total_pairs = 0, kept_pairs = 0;
@@ -69,7 +80,12 @@ public:
 
 // Computes Schwarz bounds of every pair of a basis on the device and returns
 // the sorted, screened pair list of that molecule.
-MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s);
+// decay > 0 replaces the Schwarz bound by the reference's heuristic shell-pair
+// decay indicator K_A K_B exp(-mu_min |AB|^2) (rys_engine.ipp:2205-2241) and
+// screens the pair products against decay instead of tau.
+MolPairs build_mol_pairs(const Basis& b, double tau, cudaStream_t s, double decay = 0.0);
+// Allocates the density-screen tables of a plan (idempotent).
+void ensure_density_tables(Plan2e& plan);
 
 // Builds the device plan for a set of bases (one per molecule) with their
 // already screened pair lists.

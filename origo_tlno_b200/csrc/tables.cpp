@@ -246,6 +246,59 @@ bool rys_rule_accurate(int n, double t, double* roots, double* weights) {
     return true;
 }
 
+int rys32_intervals(int n) { return static_cast<int>(std::ceil(rys_tmax(n) * kRys32PerUnit)); }
+
+std::vector<float> rys32_table(int n) {
+    constexpr int nc = kRys32Deg + 1;
+    const int nint = rys32_intervals(n);
+    std::vector<float> out(static_cast<std::size_t>(nint) * nc * 2 * n, 0.0f);
+    // Chebyshev nodes of [-1/2, 1/2] and the inverse of their Vandermonde
+    // matrix (monomials in u, lowest power first), in long double.
+    long double un[nc];
+    for (int j = 0; j < nc; ++j) un[j] = 0.5L * std::cos((2.0L * j + 1.0L) * 3.14159265358979323846264338327950288L / (2.0L * nc));
+    long double A[nc][2 * nc];
+    for (int r = 0; r < nc; ++r) {
+        long double pw = 1.0L;
+        for (int c = 0; c < nc; ++c) { A[r][c] = pw; pw *= un[r]; }
+        for (int c = 0; c < nc; ++c) A[r][nc + c] = (r == c) ? 1.0L : 0.0L;
+    }
+    for (int c = 0; c < nc; ++c) {  // Gauss-Jordan with partial pivoting
+        int piv = c;
+        for (int r = c + 1; r < nc; ++r)
+            if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+        for (int k = 0; k < 2 * nc; ++k) std::swap(A[c][k], A[piv][k]);
+        const long double d = A[c][c];
+        for (int k = 0; k < 2 * nc; ++k) A[c][k] /= d;
+        for (int r = 0; r < nc; ++r) {
+            if (r == c) continue;
+            const long double f = A[r][c];
+            for (int k = 0; k < 2 * nc; ++k) A[r][k] -= f * A[c][k];
+        }
+    }
+    const double h = 1.0 / kRys32PerUnit;
+    for (int k = 0; k < nint; ++k) {
+        double vals[nc][2 * kRysMaxN];
+        for (int j = 0; j < nc; ++j) {
+            const double T = (k + 0.5 + static_cast<double>(un[j])) * h;
+            double r[kRysMaxN], w[kRysMaxN];
+            if (!rys_rule_accurate(n, T, r, w))
+                throw std::runtime_error("tlno_gpu: Rys rule failed its moment check at N=" + std::to_string(n) +
+                                         " T=" + std::to_string(T));
+            for (int i = 0; i < n; ++i) {
+                vals[j][i] = r[i];
+                vals[j][n + i] = w[i];
+            }
+        }
+        for (int i = 0; i < 2 * n; ++i)
+            for (int c = 0; c < nc; ++c) {  // coefficient c = sum_j inv(V)[c][j] f(u_j)
+                long double acc = 0.0L;
+                for (int j = 0; j < nc; ++j) acc += A[c][nc + j] * vals[j][i];
+                out[(static_cast<std::size_t>(k) * nc + c) * 2 * n + i] = static_cast<float>(acc);
+            }
+    }
+    return out;
+}
+
 const HostTables& host_tables() {
     static std::once_flag once;
     static HostTables tabs;

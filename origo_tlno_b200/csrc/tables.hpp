@@ -33,6 +33,21 @@ struct HostTables {
     double herm_weight[kRysMaxN + 1][kRysMaxN] = {{0}};
 };
 
+// FP32 Rys tables of the mixed-precision kernels for root counts
+// 1..kRys32MaxN: on each interval [k h, (k+1) h), h = 1 / kRys32PerUnit, of
+// [0, tmax(N)) the N roots and N weights are degree-kRys32Deg polynomials in
+// u = T / h - k - 1/2 in [-1/2, 1/2), interpolating the accurate rule at the
+// Chebyshev nodes of the interval (near-minimax; error below 2e-10 times the
+// sixth derivative, far under FP32 rounding).  Record k holds
+// (kRys32Deg + 1) coefficient rows of 2N floats (N roots, then N weights),
+// lowest power first: [(k * (kRys32Deg + 1) + j) * 2N + i].  Small enough to
+// sit in shared memory (N = 3: 24.8 KB).
+constexpr int kRys32MaxN = 3;
+constexpr int kRys32PerUnit = 4;
+constexpr int kRys32Deg = 5;
+int rys32_intervals(int n);
+std::vector<float> rys32_table(int n);
+
 // Builds (once per process, thread-safe) and returns the tables.
 const HostTables& host_tables();
 

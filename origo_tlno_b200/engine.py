@@ -7,6 +7,10 @@ Names, argument meaning and error behaviour follow the reference:
 * ``build_direct_plan(basis, options)`` -- fock::build_direct_plan (:46-48).
 * ``build_coulomb_j / build_exchange_k / build_rhf_g(plan, density, options)``
   -- jk_direct.hpp:82-96; results carry ``j`` / ``k`` / ``g`` and ``M``.
+* ``build_jk_direct_for_G_rys(plan, density, options)`` --
+  fock/eri_direct_jk.hpp:36-39; ``Incremental`` -- EriDirectJKIncrementalState
+  (eri_direct_jk.hpp:41-135); ``build_eri_packed_for_G_rys(plan)`` -- the ERI
+  checksum stream (twoe_integrals.hpp:114-119).
 * ``build_one_electron_spherical_matrices(build)`` and
   ``evaluate_one_electron_matrices_sph_into(build, plan, mats)`` --
   integrals/one_electron/onee_matrices.hpp:50, 63-66.
@@ -113,7 +117,11 @@ class Context:
         N.check(N.lib().tlno_gpu_plan_profile(self.h, C.byref(p)))
         return {f: getattr(p, f) for f, _ in N.Profile._fields_}
 
-    def jk(self, density, want=("J", "K"), mixed=False, validate=True):
+    def jk(self, density, want=("J", "K"), mixed=False, validate=True,
+           options: Optional[ScreeningOptions] = None):
+        """J / K / G of a host density.  ``options`` are the reference's
+        build-time ScreeningOptions (density and FASTSCHWARZ screening of this
+        build; another integral or decay threshold re-plans)."""
         D = _f64(density)
         M = self.M
         if D.shape != (M, M):
@@ -134,7 +142,17 @@ class Context:
             flags |= N.MIXED
         if not validate:
             flags |= N.NO_VALIDATE
-        N.check(N.lib().tlno_gpu_jk(self.h, N.ptr(D), N.ptr(J), N.ptr(K), N.ptr(G), flags))
+        if options is None:
+            N.check(N.lib().tlno_gpu_jk(self.h, N.ptr(D), N.ptr(J), N.ptr(K), N.ptr(G), flags))
+        else:
+            opts = options.to_c()
+            if self.options is not None:
+                opts.mixed_threshold = self.options.mixed_threshold
+            N.check(N.lib().tlno_gpu_jk_with_options(self.h, N.ptr(D), N.ptr(J), N.ptr(K), N.ptr(G), flags,
+                                                     C.byref(opts)))
+            self.options = ScreeningOptions(options.integral_threshold, options.primitive_fastschwarz_threshold,
+                                            options.decay_threshold, options.density_threshold,
+                                            opts.mixed_threshold)
         for k, v in (("J", J), ("K", K), ("G", G)):
             if v is not None:
                 out[k] = v
@@ -143,6 +161,14 @@ class Context:
     def jk_device(self, d_density_ptr: int, d_J: int, d_K: int, mixed=False, validate=False):
         flags = N.WANT_J | N.WANT_K | N.DEVICE_PTRS | (N.MIXED if mixed else 0) | (0 if validate else N.NO_VALIDATE)
         N.check(N.lib().tlno_gpu_jk(self.h, d_density_ptr, d_J, d_K, None, flags))
+
+    def eri_checksum(self):
+        """(checksum, device ms) of the ERI stream: the sum of the canonical
+        unique spherical ERIs that pass the plan's screen."""
+        cs = C.c_double()
+        ms = C.c_double()
+        N.check(N.lib().tlno_gpu_eri_checksum(self.h, C.byref(cs), C.byref(ms)))
+        return cs.value, ms.value
 
     def graph_capture(self, d_density_ptr: int, d_J: int, d_K: int, mixed=False):
         flags = N.WANT_J | N.WANT_K | (N.MIXED if mixed else 0)
@@ -197,8 +223,8 @@ class Context:
         N.check(N.lib().tlno_gpu_set_onee_thresholds(self.h, decay_eps, nuclear_eps))
 
     # -- tuning ---------------------------------------------------------
-    def set_tuning(self, fast_bb=4, generic_bk=64, generic_warps=0, grid_mult=8):
-        t = N.Tuning(fast_bb, generic_bk, generic_warps, grid_mult)
+    def set_tuning(self, generic_bk=64, generic_warps=0, grid_mult=8):
+        t = N.Tuning(generic_bk, generic_warps, grid_mult)
         N.check(N.lib().tlno_gpu_set_tuning(self.h, C.byref(t)))
 
     def set_combo_generic(self, combo_id: int, force: bool):
@@ -285,6 +311,75 @@ class Batch:
         return N.lib().tlno_gpu_batch_stream(self.h)
 
 
+class Incremental:
+    """Incremental dP builds of G = J - K/2 (the reference's
+    EriDirectJKIncrementalState, fock/eri_direct_jk.hpp:41-135): update()
+    returns "exact_rebuild", "incremental_update" or "skipped_unchanged"."""
+
+    STATUS = {1: "exact_rebuild", 2: "incremental_update", 3: "skipped_unchanged", 0: "uninitialized"}
+
+    def __init__(self, context: Context, base_options: Optional[ScreeningOptions] = None,
+                 exact_rebuild_interval: int = 8, delta_density_threshold: float = 0.0,
+                 use_first_delta_density_threshold: bool = False, first_delta_density_threshold: float = 0.0):
+        base = (base_options or ScreeningOptions()).to_c()
+        o = N.IncrementalOptions(base, exact_rebuild_interval, delta_density_threshold,
+                                 1 if use_first_delta_density_threshold else 0, first_delta_density_threshold)
+        h = C.c_void_p()
+        N.check(N.lib().tlno_gpu_incremental_create(context.h, C.byref(o), C.byref(h)))
+        self.h = h
+        self.context = context
+        self.M = context.M
+
+    def close(self):
+        if getattr(self, "h", None):
+            N.lib().tlno_gpu_incremental_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update(self, density, force_exact_rebuild: bool = False, mixed: bool = False) -> str:
+        D = _f64(density)
+        if D.shape != (self.M, self.M):
+            raise TlnoError(N.E_INVALID, "eri_ao_tensor_hgp: incremental density must be spherical M x M row-major.")
+        rc = N.check(N.lib().tlno_gpu_incremental_update(self.h, N.ptr(D), 1 if force_exact_rebuild else 0,
+                                                         N.MIXED if mixed else 0))
+        return self.STATUS[rc]
+
+    def update_device(self, d_density: int, force_exact_rebuild: bool = False, mixed: bool = False) -> str:
+        rc = N.check(N.lib().tlno_gpu_incremental_update(self.h, d_density, 1 if force_exact_rebuild else 0,
+                                                         N.DEVICE_PTRS | (N.MIXED if mixed else 0)))
+        return self.STATUS[rc]
+
+    def g(self) -> np.ndarray:
+        G = np.empty((self.M, self.M))
+        N.check(N.lib().tlno_gpu_incremental_g(self.h, N.ptr(G), 0))
+        return G
+
+    def density(self) -> np.ndarray:
+        D = np.empty((self.M, self.M))
+        N.check(N.lib().tlno_gpu_incremental_density(self.h, N.ptr(D), 0))
+        return D
+
+    def info(self) -> dict:
+        i = N.IncrementalInfo()
+        N.check(N.lib().tlno_gpu_incremental_info_get(self.h, C.byref(i)))
+        d = {f: getattr(i, f) for f, _ in N.IncrementalInfo._fields_}
+        d["last_status"] = self.STATUS[d["last_status"]]
+        return d
+
+    def reset(self):
+        N.check(N.lib().tlno_gpu_incremental_reset(self.h))
+
+    def fail_next_update(self, stage: int):
+        """Testing hook: the next update fails at `stage` (1 before the build,
+        2 before the commit)."""
+        N.check(N.lib().tlno_gpu_incremental_fail_next_update(self.h, stage))
+
+
 # ---------------- reference-named facade ----------------
 
 @dataclass
@@ -316,25 +411,26 @@ def build_direct_plan(basis: Molecule, options: Optional[ScreeningOptions] = Non
     return DirectPlan(ctx, ctx.profile())
 
 
-def _check_options(plan: DirectPlan, options: Optional[ScreeningOptions]):
-    if options is not None and plan.context.options is not None and \
-            options.integral_threshold != plan.context.options.integral_threshold:
-        plan.context.plan(options)
-
-
 def build_coulomb_j(plan: DirectPlan, density, options: Optional[ScreeningOptions] = None) -> CoulombJResult:
-    _check_options(plan, options)
-    return CoulombJResult(plan.context.jk(density, want=("J",))["J"], plan.context.M)
+    return CoulombJResult(plan.context.jk(density, want=("J",), options=options)["J"], plan.context.M)
 
 
 def build_exchange_k(plan: DirectPlan, density, options: Optional[ScreeningOptions] = None) -> ExchangeKResult:
-    _check_options(plan, options)
-    return ExchangeKResult(plan.context.jk(density, want=("K",))["K"], plan.context.M)
+    return ExchangeKResult(plan.context.jk(density, want=("K",), options=options)["K"], plan.context.M)
 
 
 def build_rhf_g(plan: DirectPlan, density, options: Optional[ScreeningOptions] = None) -> DirectResult:
-    _check_options(plan, options)
-    return DirectResult(plan.context.jk(density, want=("G",))["G"], plan.context.M)
+    return DirectResult(plan.context.jk(density, want=("G",), options=options)["G"], plan.context.M)
+
+
+def build_jk_direct_for_G_rys(plan: DirectPlan, density, options: Optional[ScreeningOptions] = None) -> DirectResult:
+    """Compatibility endpoint (fock/eri_direct_jk.hpp:36-39): G = J - K/2."""
+    return build_rhf_g(plan, density, options)
+
+
+def build_eri_packed_for_G_rys(plan: DirectPlan) -> float:
+    """ERI checksum stream of the plan (twoe_integrals.hpp:114-119)."""
+    return plan.context.eri_checksum()[0]
 
 
 _ONEE = {"enabled": True, "decay": 1.0e-15, "nuclear": 1.0e-15}

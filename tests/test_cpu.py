@@ -231,3 +231,57 @@ def test_replicas_gloo_world_size_2(tmp_path):
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=240, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count("ok") == 2, r.stdout
+
+
+# ---------------- oracle harness: screening, incremental state, ERI stream ----------------
+
+@pytest.fixture(scope="module")
+def refw3():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("compiled reference not built here")
+    mol = M.water_cluster(3, seed=5)
+    return ref, mol, ref.RefBasis(mol)
+
+
+def test_ref_harness_screening_entries(refw3):
+    ref, mol, rb = refw3
+    D = M.random_density(mol.n_sph, 6, seed=11)
+    base = rb.jk(D, schwarz=1e-12)
+    same = rb.jk_opts(D, schwarz=1e-12)
+    for k in ("J", "K", "G"):
+        assert np.array_equal(base[k], same[k])
+    # the compatibility endpoint builds the same G as the facade
+    assert np.max(np.abs(rb.jk_compat(D, schwarz=1e-12) - base["G"])) < 1e-13
+    # a density threshold removes quartets (results change, stay close)
+    scr = rb.jk_opts(D, schwarz=1e-12, density_threshold=1e-7)
+    d = np.max(np.abs(scr["J"] - base["J"]))
+    assert 0.0 < d < 1e-5
+    with pytest.raises(RuntimeError, match="heuristic decay"):
+        rb.jk_opts(D, schwarz=0.0, decay=1e-10, density_threshold=1e-9)
+    with pytest.raises(RuntimeError, match="exactly one shell-level metric"):
+        rb.jk_opts(D, schwarz=1e-12, decay=1e-10)
+    cs, secs = rb.eri_checksum(schwarz=0.0)
+    assert np.isfinite(cs) and secs >= 0.0
+
+
+def test_ref_harness_incremental_state(refw3):
+    ref, mol, rb = refw3
+    D0 = M.random_density(mol.n_sph, 6, seed=12)
+    D1 = D0 + 1e-3 * M.random_density(mol.n_sph, 6, seed=13)
+    st = ref.RefIncremental(rb, schwarz=1e-12, exact_rebuild_interval=2)
+    r0 = st.update(D0)
+    assert r0["status"] == "exact_rebuild" and r0["counters"] == [1, 1, 0, 0]
+    assert np.max(np.abs(r0["G"] - rb.jk(D0, schwarz=1e-12)["G"])) < 1e-13
+    r1 = st.update(D1)
+    assert r1["status"] == "incremental_update" and r1["counters"] == [2, 1, 1, 0]
+    assert np.max(np.abs(r1["G"] - rb.jk(D1, schwarz=1e-12)["G"])) < 1e-12
+    r2 = st.update(D1)
+    assert r2["status"] == "skipped_unchanged" and r2["counters"] == [3, 1, 1, 1]
+
+
+def test_ref_harness_components_round_trip(refw3):
+    ref, mol, rb = refw3
+    centers, ang, nprim, exps, coefs = rb.components()
+    assert len(nprim) == mol.n_cart == rb.n_cart
+    assert np.all(ang.sum(axis=1) >= 0) and len(exps) == int(nprim.sum()) == len(coefs)
