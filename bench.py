@@ -224,6 +224,107 @@ def _profiled_traffic(workload, tag):
     return float(v) if v is not None else None
 
 
+def _host_cpu():
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cores": os.cpu_count(), "cores_usable": _cpu_count()}
+
+
+def _incremental_leg(ctx, Ds, tau, J64, K64):
+    """The density sequence through the incremental state: time per update
+    (host wall clock around each update call, which ends with the device work
+    done) and the final G against the full FP64 build of the last density."""
+    import torch
+    from origo_tlno_b200 import engine as E
+    interval = len(Ds)  # one exact build, then dP builds only
+    st = E.Incremental(ctx, E.ScreeningOptions(integral_threshold=tau), exact_rebuild_interval=interval,
+                       delta_density_threshold=tau)
+    times, statuses = [], []
+    for D in Ds:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        statuses.append(st.update_device(D.data_ptr()))
+        times.append(time.perf_counter() - t0)
+    G = torch.tensor(st.g(), device=Ds[-1].device)
+    G64 = J64 - 0.5 * K64
+    info = st.info()
+    st.close()
+    inc = [t for t, s in zip(times, statuses) if s == "incremental_update"]
+    exa = [t for t, s in zip(times, statuses) if s == "exact_rebuild"]
+    return {"updates": len(Ds), "exact_rebuilds": info["exact_rebuilds"],
+            "incremental_updates": info["incremental_updates"],
+            "ms_per_incremental_update": 1e3 * float(np.mean(inc)) if inc else None,
+            "ms_per_exact_rebuild": 1e3 * float(np.mean(exa)) if exa else None,
+            "ms_total": 1e3 * float(np.sum(times)),
+            "delta_density_threshold": tau, "exact_rebuild_interval": interval,
+            "final_max_abs_dG_vs_full_fp64": float((G - G64).abs().max().item()),
+            "final_abs_dE_vs_full_fp64": abs(float(torch.sum(Ds[-1] * (G - G64)).item()))}
+
+
+def _checksum_leg(ctx, quartets):
+    """ERI-only throughput: the checksum stream over the plan (no J/K)."""
+    ctx.eri_checksum()  # warm-up
+    cs, ms = ctx.eri_checksum()
+    return {"checksum": cs, "ms": ms, "value": quartets / (ms * 1e-3), "unit": UNIT,
+            "note": "sum of the canonical unique spherical ERIs of the plan (build_eri_packed_for_G_rys)"}
+
+
+def _onee_leg(ctx, mol, with_cpu):
+    """One-electron S, T, V: GPU time of the workload (device buffers,
+    CUDA events) and the reference on a bounded sample with every core."""
+    import torch
+    from origo_tlno_b200 import _native as N
+    dev = torch.device("cuda", ctx.device)
+    M = ctx.M
+    bufs = [torch.empty(M, M, dtype=torch.float64, device=dev) for _ in range(3)]
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    run = lambda: N.check(N.lib().tlno_gpu_onee(ctx.h, bufs[0].data_ptr(), bufs[1].data_ptr(), bufs[2].data_ptr(),
+                                                1, N.DEVICE_PTRS))
+    run()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            run()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    out = {"gpu_ms": e0.elapsed_time(e1) / 3, "M": M, "nuclei": int(len(mol.charges))}
+    if with_cpu:
+        try:
+            from oracle import ref
+            sample = MOL.water_cluster(40, seed=5)
+            rb = ref.RefBasis(sample)
+            ref.set_threads(_cpu_count())
+            t0 = time.perf_counter()
+            rb.onee(screening=True)
+            out["cpu_baseline"] = {"ms": 1e3 * (time.perf_counter() - t0), "cores": _cpu_count(),
+                                   "kind": "reference", "sample": "40-water sub-cluster (M=960), S+T+V"}
+            gctx = E_context(sample)
+            gctx.onee()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            gctx.onee()
+            out["gpu_ms_same_sample_host_call"] = 1e3 * (time.perf_counter() - t0)
+            gctx.close()
+        except Exception as e:  # the reference oracle may be absent
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    return out
+
+
+def E_context(mol):
+    from origo_tlno_b200 import engine as E
+    return E.Context(mol)
+
+
 def run_batch(args):
     """cfg3: 256 molecules (3-30 atoms, cfg1 basis recipe) in one batch --
     one launch per quartet class over all molecules, the whole build one CUDA
@@ -381,7 +482,8 @@ def run_native(args):
     e2e_times = []
     for r in range(max(2, min(3, args.steps))):
         t0 = time.time()
-        out = ctx.jk(Dh, want=("J", "K"), mixed=True, validate=False)
+        # the density contract is checked on every call, as the reference does
+        out = ctx.jk(Dh, want=("J", "K"), mixed=True, validate=True)
         e2e_times.append(time.time() - t0)
     e2e_t = float(np.median(e2e_times[1:] if len(e2e_times) > 1 else e2e_times))
     e2e = {"value": ws * quartets / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(Dh.nbytes),
@@ -412,9 +514,23 @@ def run_native(args):
             secs, desc, smol, stau = _reference_sample(args.config)
             q = _count_quartets(smol, stau)
             cpu = {"value": q / secs, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": desc + f" ({q} quartets, {secs:.2f} s)"}
+                   "sample": desc + f" ({q} quartets, {secs:.2f} s)", "host": _host_cpu(),
+                   "route": "AVX2 (-march=x86-64-v3), the reference's legacy tuned route; its G/K endpoints "
+                            "refuse more than one OpenMP thread"}
         except Exception as e:  # the reference oracle may be absent
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    # incremental dP builds over the same density sequence (the reference's
+    # EriDirectJKIncrementalState form): one exact build, then every changed
+    # density as dP under the density screen at the Schwarz threshold
+    incremental = None
+    if not args.no_extra:
+        incremental = _incremental_leg(ctx, Ds, tau, J64, K64)
+        # ERI checksum stream (the reference's twoe_timing endpoint) on the plan
+        checksum_leg = _checksum_leg(ctx, quartets)
+        onee_leg = _onee_leg(ctx, mol, rank == 0 and not args.no_cpu_baseline)
+    else:
+        checksum_leg = onee_leg = None
 
     clocks = sampler.summary()
     res = {
@@ -443,6 +559,7 @@ def run_native(args):
                      "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu "
                                        "capture of the same class and workload (profiles/)"},
         "e2e": e2e, "gpu_launches": launches * steps,
+        "incremental": incremental, "eri_checksum_stream": checksum_leg, "one_electron": onee_leg,
         "clocks": clocks, "wall_s_timed": t_wall,
         "cpu_baseline": cpu,
     }
@@ -463,6 +580,8 @@ def main():
     ap.add_argument("--config", default="cfg4")
     ap.add_argument("--mixed-threshold", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the incremental, ERI-stream and one-electron legs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep --mixed-threshold instead of autotuning the split threshold")
     args = ap.parse_args()

@@ -32,6 +32,15 @@ SRCS=(
   integrals/one_electron/onee_integrals.cpp
   integrals/one_electron/onee_matrices.cpp
   integrals/two_electron/fock/jk_direct.cpp
+  core/basis/basis_general.cpp
+  core/basis/get_sto3g_params.cpp
+  core/basis/get_4_31g_params.cpp
+  core/basis/get_6_31g_params.cpp
+  core/basis/get_6_31g_d_params.cpp
+  core/basis/get_6_31g_dp_params.cpp
+  core/basis/get_def2_svp_params.cpp
+  core/basis/get_def2_tzvp_params.cpp
+  benchmarks/common/molecule_io.cpp
 )
 pids=()
 objs=()
@@ -43,12 +52,14 @@ for s in "${SRCS[@]}"; do
     pids+=($!)
   fi
 done
-H="$OBJ/ref_harness.o"
-objs+=("$H")
-if [ ! -f "$H" ] || [ "$HERE/ref_harness.cpp" -nt "$H" ]; then
-  "$CXX" "${FLAGS[@]}" -c "$HERE/ref_harness.cpp" -o "$H" &
-  pids+=($!)
-fi
+for h in ref_harness ref_frontend; do
+  H="$OBJ/$h.o"
+  objs+=("$H")
+  if [ ! -f "$H" ] || [ "$HERE/$h.cpp" -nt "$H" ]; then
+    "$CXX" "${FLAGS[@]}" -c "$HERE/$h.cpp" -o "$H" &
+    pids+=($!)
+  fi
+done
 for p in "${pids[@]}"; do wait "$p"; done
 "$CXX" -shared -fopenmp -o "$OUT/libtlno_ref.so" "${objs[@]}"
 echo "build_ref: wrote $OUT/libtlno_ref.so"

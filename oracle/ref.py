@@ -260,3 +260,85 @@ class RefIncremental:
             self.close()
         except Exception:
             pass
+
+
+# ---------------- front end (oracle/ref_frontend.cpp) ----------------
+
+def _front():
+    L = lib()
+    if not getattr(L, "_front_ready", False):
+        vp = C.c_void_p
+        L.ref_frontend_last_error.restype = C.c_char_p
+        L.ref_read_inp.argtypes = [C.c_char_p, C.c_int, vp, vp, vp, vp, vp]
+        L.ref_basis_general.argtypes = [C.c_int, vp, vp, C.c_int, C.c_char_p, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.ref_raw_atom_basis.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, vp, vp, vp, vp]
+        L.ref_parse_basis_kind.argtypes = [C.c_char_p]
+        L._front_ready = True
+    return L
+
+
+def _fchk(rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + _front().ref_frontend_last_error().decode())
+
+
+def read_inp(path):
+    """(symbols, coords_bohr, charge, multiplicity) through read_inp_file."""
+    n = C.c_int()
+    ch = C.c_int()
+    mu = C.c_int()
+    _fchk(_front().ref_read_inp(path.encode(), 0, C.byref(n), None, None, C.byref(ch), C.byref(mu)))
+    sym = C.create_string_buffer(8 * n.value)
+    xyz = np.empty((n.value, 3))
+    _fchk(_front().ref_read_inp(path.encode(), n.value, C.byref(n), sym, xyz.ctypes.data, C.byref(ch), C.byref(mu)))
+    raw = sym.raw
+    symbols = [raw[8 * a:8 * a + 8].split(b"\0")[0].decode() for a in range(n.value)]
+    return symbols, xyz, ch.value, mu.value
+
+
+def basis_general(symbols, coords, charge, basis):
+    """Component records, nuclear charges and electron count of
+    build_basis_general."""
+    n = len(symbols)
+    sym = C.create_string_buffer(b"".join(s.encode()[:7].ljust(8, b"\0") for s in symbols), 8 * n)
+    xyz = np.ascontiguousarray(coords, dtype=np.float64)
+    nc = C.c_int()
+    npr = C.c_int()
+    el = C.c_int()
+    Z = np.empty(n, dtype=np.int32)
+    _fchk(_front().ref_basis_general(n, sym, xyz.ctypes.data, charge, basis.encode(), C.byref(nc), C.byref(npr),
+                                     None, None, None, None, None, Z.ctypes.data, C.byref(el)))
+    centers = np.empty((nc.value, 3))
+    ang = np.empty((nc.value, 3), dtype=np.int32)
+    nprim = np.empty(nc.value, dtype=np.int32)
+    exps = np.empty(npr.value)
+    coefs = np.empty(npr.value)
+    _fchk(_front().ref_basis_general(n, sym, xyz.ctypes.data, charge, basis.encode(), C.byref(nc), C.byref(npr),
+                                     centers.ctypes.data, ang.ctypes.data, nprim.ctypes.data, exps.ctypes.data,
+                                     coefs.ctypes.data, Z.ctypes.data, C.byref(el)))
+    return (centers, ang, nprim, exps, coefs), Z, el.value
+
+
+def raw_atom_basis(symbol, basis):
+    """(charge, [(ang, exponents, raw coefficients)]) of the reference's
+    per-element table."""
+    ch = C.c_int()
+    nr = C.c_int()
+    npr = C.c_int()
+    _fchk(_front().ref_raw_atom_basis(symbol.encode(), basis.encode(), C.byref(ch), C.byref(nr), C.byref(npr),
+                                      None, None, None, None))
+    ang = np.empty((nr.value, 3), dtype=np.int32)
+    nprim = np.empty(nr.value, dtype=np.int32)
+    exps = np.empty(npr.value)
+    coefs = np.empty(npr.value)
+    _fchk(_front().ref_raw_atom_basis(symbol.encode(), basis.encode(), C.byref(ch), C.byref(nr), C.byref(npr),
+                                      ang.ctypes.data, nprim.ctypes.data, exps.ctypes.data, coefs.ctypes.data))
+    out, p = [], 0
+    for k in range(nr.value):
+        out.append((tuple(int(v) for v in ang[k]), exps[p:p + nprim[k]].copy(), coefs[p:p + nprim[k]].copy()))
+        p += nprim[k]
+    return ch.value, out
+
+
+def parse_basis_kind_ok(name):
+    return _front().ref_parse_basis_kind(name.encode()) == 0

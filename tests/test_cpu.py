@@ -285,3 +285,89 @@ def test_ref_harness_components_round_trip(refw3):
     centers, ang, nprim, exps, coefs = rb.components()
     assert len(nprim) == mol.n_cart == rb.n_cart
     assert np.all(ang.sum(axis=1) >= 0) and len(exps) == int(nprim.sum()) == len(coefs)
+
+
+# ---------------- front end: .inp reader and named bases ----------------
+
+REF_ROOT = os.environ.get("TLNO_REFERENCE_ROOT", "/root/reference")
+MOLDIR = os.path.join(REF_ROOT, "test_molecules")
+
+
+def _gaussian94_from_reference(ref, symbols, basis):
+    """A Gaussian94 basis file written from the reference's raw tables (one
+    contracted shell per run of Cartesian components of one L)."""
+    names = "SPDFG"
+    out = []
+    for sym in sorted(set(symbols)):
+        _, raw = ref.raw_atom_basis(sym, basis)
+        out.append(f"{sym}     0")
+        for ang, e, c in raw:
+            L = sum(ang)
+            if ang != (L, 0, 0):
+                continue  # the first component of each shell carries the shell
+            out.append(f"{names[L]}   {len(e)}   1.00")
+            out += [f"  {float(x)!r}  {float(y)!r}" for x, y in zip(e, c)]
+        out.append("****")
+    return "\n".join(out) + "\n"
+
+
+@pytest.mark.skipif(not os.path.isdir(MOLDIR), reason="reference test molecules not present")
+def test_frontend_reader_matches_reference_on_every_input():
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("compiled reference not built here")
+    from origo_tlno_b200 import frontend as F
+    files = sorted(f for f in os.listdir(MOLDIR) if f.endswith(".inp"))
+    assert len(files) >= 30
+    for f in files:
+        path = os.path.join(MOLDIR, f)
+        mine = F.read_inp_file(path)
+        sym, xyz, ch, mu = ref.read_inp(path)
+        assert mine.symbols == sym, f
+        assert np.array_equal(np.array(mine.coords_bohr), xyz), f
+        assert (mine.charge, mine.multiplicity) == (ch, mu), f
+
+
+def test_frontend_reader_errors(tmp_path):
+    from origo_tlno_b200 import frontend as F
+    p = tmp_path / "m.inp"
+    p.write_text("* xyz 0 1\nO 0 0 0\n")
+    with pytest.raises(F.FrontendError, match="Unterminated xyz block"):
+        F.read_inp_file(str(p))
+    p.write_text("* xyz 0 0\nO 0 0 0\n*\n")
+    with pytest.raises(F.FrontendError, match="multiplicity must be at least one"):
+        F.read_inp_file(str(p))
+    p.write_text("* xyz 0 1\nO 0 nan 0\n*\n")
+    with pytest.raises(F.FrontendError, match="bad coordinate line 2"):
+        F.read_inp_file(str(p))
+    p.write_text("O 0 0 0\n")
+    with pytest.raises(F.FrontendError, match="Missing"):
+        F.read_inp_file(str(p))
+    with pytest.raises(F.FrontendError, match="Unsupported basis set: cc-pvdz"):
+        F.parse_basis_kind("cc-pvdz")
+    assert F.parse_basis_kind("6-31G**") == "6-31g(d,p)" and F.parse_basis_kind("def2-dzvp") == "def2-svp"
+
+
+@pytest.mark.skipif(not os.path.isdir(MOLDIR), reason="reference test molecules not present")
+@pytest.mark.parametrize("name,basis", [("h2o", "def2-svp"), ("glucose", "def2-svp"), ("caffeine", "def2-tzvp"),
+                                        ("benzene", "6-31g**"), ("co", "sto-3g")])
+def test_frontend_named_basis_matches_build_basis_general(name, basis):
+    """A Gaussian94 file of the named basis, read by the front end and
+    normalised by make_shell, reproduces the reference's build_basis_general
+    component records (so the engine sees the reference's basis)."""
+    from oracle import ref
+    if not ref.available():
+        pytest.skip("compiled reference not built here")
+    from origo_tlno_b200 import frontend as F
+    for kind in ("sto-3g", "def2-svp", "def2-tzvp", "6-31g**"):
+        assert ref.parse_basis_kind_ok(kind)
+    inp = F.read_inp_file(os.path.join(MOLDIR, name + ".inp"))
+    spec = F.molecule_spec(inp)
+    lib = F.load_basis_library(_gaussian94_from_reference(ref, spec.symbols, basis))
+    mol, electrons = F.build_basis_general(spec, lib, name=name)
+    (c_ref, a_ref, n_ref, e_ref, k_ref), Z, el_ref = ref.basis_general(spec.symbols, spec.coords, spec.charge, basis)
+    assert electrons == el_ref and np.array_equal(mol.charges, Z)
+    c, a, n, e, k = ref.RefBasis(mol).components()
+    assert np.array_equal(a, a_ref) and np.array_equal(n, n_ref)
+    assert np.array_equal(c, c_ref) and np.array_equal(e, e_ref)
+    assert np.max(np.abs(k - k_ref) / np.abs(k_ref)) < 1e-14
