@@ -266,8 +266,12 @@ int tlno_gpu_schwarz(const tlno_gpu_context* ctx, double* out);
  * n x (maxn+1)).  Reference: core/math/general_math.hpp:6-22. */
 int tlno_gpu_boys(int device, int n, int maxn, const double* x, double* out);
 /* Device Rys roots (t^2) and weights for nroots at n arguments (host
- * buffers, n x nroots each); fp32 selects the single-precision tables.
- * Reference: rys_roots_weights (rys_engine.ipp:3823-3838). */
+ * buffers, n x nroots each).  Reference: rys_roots_weights
+ * (rys_engine.ipp:3823-3838).  fp32 selects the evaluation path of the
+ * kernels: 0 = FP64 tables (the reference's 0.01-grid interpolant),
+ * 1 = FP32 tables, 2 = the FP32 interval polynomials of the mixed-precision
+ * kernels (nroots <= 3), 3 = the FP64 closed forms from Boys values of the
+ * N <= 2 kernels (nroots <= 2). */
 int tlno_gpu_rys(int device, int n, int nroots, const double* T, double* roots, double* weights,
                  int fp32);
 

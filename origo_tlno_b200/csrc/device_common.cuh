@@ -31,7 +31,14 @@ struct DevTables {
     // (lowest power of u = 4T - k - 1/2 first); staged in shared memory.
     const float* rys32[4];
     int rys32_nint[4];
+    // FP64 Boys interval polynomials of F_{2N-1} for N = 1, 2: interval k of
+    // width 1/4 holds 10 coefficients (lowest power of u = 4T - k - 1/2
+    // first); staged in shared memory by the N <= 2 FP64 kernels.
+    const double* boys_iv[3];
+    int boys_iv_nint[3];
 };
+constexpr int kBoysIvCoefDev = 10;
+constexpr int kBoysIvPerUnitDev = 4;
 constexpr int kRys32PerUnitDev = 4;
 constexpr int kRys32CoefDev = 6;
 
@@ -193,6 +200,67 @@ __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
         v = v * t + c[1][i];
         v = v * t + c[0][i];
         if (i < N) root[i] = v; else weight[i - N] = v;
+    }
+}
+
+// FP64 roots and weights for N <= 2 from Boys values (the Rys quadrature
+// moments mu_k = F_k(T)): F_{2N-1} from the shared-memory interval
+// polynomials, F_{2N-2} .. F_0 by the downward recursion
+// F_{n-1} = (2T F_n + e^{-T}) / (2n - 1), then the Gauss rule of the moments
+// in closed form -- N = 1: t^2 = F_1 / F_0, w = F_0; N = 2: the eigenpairs of
+// the 2 x 2 Jacobi matrix of the monic recurrence (a0 = mu1/mu0,
+// b1 = (mu2 - a0 mu1)/mu0, a1 = (mu3 - a0 mu2)/(mu2 - a0 mu1) - a0), weights
+// mu0 b1 / (b1 + (t^2 - a0)^2).  Above tmax(N) the Hermite asymptotic form,
+// as rys_roots_all.
+template <int N>
+__device__ __forceinline__ void rys_roots_boys(double T, const double* __restrict__ table, double* root,
+                                               double* weight) {
+    static_assert(N == 1 || N == 2, "closed forms for one or two roots");
+    if (T >= c_tabs.tmax[N]) {
+        const double inv = 1.0 / T;
+        const double sinv = sqrt(inv);
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+            root[i] = c_tabs.h2[N][i] * inv;
+            weight[i] = c_tabs.hw[N][i] * sinv;
+        }
+        return;
+    }
+    const double x = T * double(kBoysIvPerUnitDev);
+    const int k = static_cast<int>(x);
+    const double u = x - double(k) - 0.5;
+    const double2* rec = reinterpret_cast<const double2*>(table + k * kBoysIvCoefDev);
+    double c[kBoysIvCoefDev];
+#pragma unroll
+    for (int j = 0; j < kBoysIvCoefDev / 2; ++j) {
+        const double2 v = rec[j];
+        c[2 * j] = v.x;
+        c[2 * j + 1] = v.y;
+    }
+    double F[2 * N];
+    double v = c[kBoysIvCoefDev - 1];
+#pragma unroll
+    for (int j = kBoysIvCoefDev - 2; j >= 0; --j) v = fma(v, u, c[j]);
+    F[2 * N - 1] = v;
+    const double e = exp(-T), t2 = T + T;
+#pragma unroll
+    for (int n = 2 * N - 1; n >= 1; --n) F[n - 1] = fma(t2, F[n], e) * (1.0 / (2 * n - 1));
+    if constexpr (N == 1) {
+        root[0] = F[1] / F[0];
+        weight[0] = F[0];
+    } else {
+        const double a0 = F[1] / F[0];
+        const double s1 = fma(-a0, F[1], F[2]);
+        const double s2 = fma(-a0, F[2], F[3]);
+        const double a1 = s2 / s1 - a0;
+        const double b1 = s1 / F[0];
+        const double half = 0.5 * (a0 + a1), diff = 0.5 * (a0 - a1);
+        const double disc = sqrt(fma(diff, diff, b1));
+        root[0] = half - disc;
+        root[1] = half + disc;
+        const double d0 = root[0] - a0, d1 = root[1] - a0;
+        weight[0] = F[0] * b1 / fma(d0, d0, b1);
+        weight[1] = F[0] * b1 / fma(d1, d1, b1);
     }
 }
 

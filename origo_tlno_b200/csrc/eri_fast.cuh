@@ -196,7 +196,11 @@ struct QuartetGeom {
 // Phase 1 + 2 for slice G (rows ia = G, G+TPQ, ...).
 template <typename R, int LA, int LB, int LC, int LD, int G>
 __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
-                                           double fs_thr2, const float* rtab, R* __restrict__ ks) {
+                                           double fs_thr2, const void* rtab_v, R* __restrict__ ks) {
+    // shared-memory root tables: FP32 interval polynomials (FP32, N <= 3) or
+    // FP64 Boys interval polynomials (FP64, N <= 2)
+    const float* rtab = static_cast<const float*>(rtab_v);
+    const double* rtab64 = static_cast<const double*>(rtab_v);
     using S = FastShape<LA, LB, LC, LD>;
     constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
     R acc[ROWS > 0 ? ROWS : 1][S::NCS];
@@ -272,6 +276,9 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
                         rt[r] = R(rd[r]);
                         wt[r] = R(wd[r]);
                     }
+                } else if constexpr (S::N <= 2) {
+                    // closed forms from Boys values, no table gather
+                    rys_roots_boys<S::N>(Targ, rtab64, rt, wt);
                 } else {
                     rys_roots_all<R, S::N>(Targ, rt, wt);
                 }
@@ -341,7 +348,7 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
 template <typename R, int LA, int LB, int LC, int LD, int G = 0>
 __device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, int bra, int ket, bool active,
-                                                    const QuartetGeom& q, double fs_thr2, const float* rtab,
+                                                    const QuartetGeom& q, double fs_thr2, const void* rtab,
                                                     R* ks) {
     using S = FastShape<LA, LB, LC, LD>;
     if constexpr (G < S::TPQ) {
@@ -386,12 +393,20 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     const int bar_id = 1 + grp, bar_n = 32 * S::TPQ;
     // FP32 kernels with N <= 3 stage their Rys interval polynomials in shared
     // memory behind the row-exchange buffer.
-    const float* rtab = nullptr;
+    const void* rtab = nullptr;
     if constexpr (std::is_same<R, float>::value && S::N <= 3) {
         float* t = reinterpret_cast<float*>(fast_smem + S::SMEM_DOUBLES);
         const int n4 = c_tabs.rys32_nint[S::N] * (kRys32CoefDev * 2 * S::N) / 4;
         const float4* src = reinterpret_cast<const float4*>(c_tabs.rys32[S::N]);
         for (int i = threadIdx.x; i < n4; i += blockDim.x) reinterpret_cast<float4*>(t)[i] = __ldg(src + i);
+        __syncthreads();
+        rtab = t;
+    } else if constexpr (std::is_same<R, double>::value && S::N <= 2) {
+        // FP64 Boys interval polynomials for the closed-form roots
+        double* t = fast_smem + S::SMEM_DOUBLES;
+        const int n2 = c_tabs.boys_iv_nint[S::N] * kBoysIvCoefDev / 2;
+        const double2* src = reinterpret_cast<const double2*>(c_tabs.boys_iv[S::N]);
+        for (int i = threadIdx.x; i < n2; i += blockDim.x) reinterpret_cast<double2*>(t)[i] = __ldg(src + i);
         __syncthreads();
         rtab = t;
     }

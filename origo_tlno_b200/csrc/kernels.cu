@@ -175,6 +175,32 @@ __global__ void rys_test_kernel(const double* T, int n, int nroots, double* root
     }
 }
 
+// Test hook of the shared-memory root paths, reading the tables from global
+// memory: mode 2 = FP32 interval polynomials (N <= 3), mode 3 = FP64 closed
+// forms from the Boys interval polynomials (N <= 2).
+template <int N>
+__global__ void rys_interval_test_kernel(const double* T, int n, int mode, double* roots, double* weights) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (mode == 2) {
+        float r[N], w[N];
+        rys_roots_smem32<N>(float(T[i]), c_tabs.rys32[N], r, w);
+        for (int k = 0; k < N; ++k) {
+            roots[(long long)i * N + k] = r[k];
+            weights[(long long)i * N + k] = w[k];
+        }
+    } else {
+        if constexpr (N <= 2) {
+            double r[N], w[N];
+            rys_roots_boys<N>(T[i], c_tabs.boys_iv[N], r, w);
+            for (int k = 0; k < N; ++k) {
+                roots[(long long)i * N + k] = r[k];
+                weights[(long long)i * N + k] = w[k];
+            }
+        }
+    }
+}
+
 __global__ void absmax_kernel(const double* x, long long n, double* out) {
     __shared__ double red[32];
     double m = 0.0;
@@ -410,6 +436,10 @@ void ensure_device_tables() {
         t.rys32[n] = upload(rys32_table(n));
         t.rys32_nint[n] = rys32_intervals(n);
     }
+    for (int n = 1; n <= 2; ++n) {
+        t.boys_iv[n] = upload(boys_iv_table(n));
+        t.boys_iv_nint[n] = boys_iv_intervals(n);
+    }
     CartTable ct{};
     build_cart(ct);
     C2STable c2s{};
@@ -632,6 +662,17 @@ void launch_boys_test(const double* x, int n, int maxn, double* out, cudaStream_
 
 void launch_rys_test(const double* t, int n, int nroots, int fp32, double* roots, double* weights,
                      cudaStream_t s) {
+    if (fp32 >= 2) {
+        const int g = (n + 127) / 128;
+        switch (nroots) {
+            case 1: rys_interval_test_kernel<1><<<g, 128, 0, s>>>(t, n, fp32, roots, weights); break;
+            case 2: rys_interval_test_kernel<2><<<g, 128, 0, s>>>(t, n, fp32, roots, weights); break;
+            case 3: rys_interval_test_kernel<3><<<g, 128, 0, s>>>(t, n, fp32, roots, weights); break;
+            default: break;
+        }
+        TLNO_CUDA(cudaGetLastError());
+        return;
+    }
     if (fp32)
         rys_test_kernel<float><<<(n + 127) / 128, 128, 0, s>>>(t, n, nroots, roots, weights);
     else

@@ -501,9 +501,15 @@ def boys(x, maxn: int, device: int = 0) -> np.ndarray:
     return out
 
 
-def rys_roots(T, nroots: int, fp32: bool = False, device: int = 0):
+RYS_PATHS = {"fp64_table": 0, "fp32_table": 1, "fp32_interval": 2, "fp64_boys": 3}
+
+
+def rys_roots(T, nroots: int, fp32: bool = False, device: int = 0, path: Optional[str] = None):
+    """Device Rys roots and weights; ``path`` selects one of the kernels'
+    evaluation paths (RYS_PATHS), default the FP64 (or FP32) tables."""
     T = _f64(np.atleast_1d(T))
     r = np.empty((len(T), nroots))
     w = np.empty((len(T), nroots))
-    N.check(N.lib().tlno_gpu_rys(device, len(T), nroots, N.ptr(T), N.ptr(r), N.ptr(w), 1 if fp32 else 0))
+    mode = RYS_PATHS[path] if path else (1 if fp32 else 0)
+    N.check(N.lib().tlno_gpu_rys(device, len(T), nroots, N.ptr(T), N.ptr(r), N.ptr(w), mode))
     return r, w

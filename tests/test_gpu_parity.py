@@ -51,11 +51,36 @@ def test_rys_roots_match_reference(n):
     assert _maxabs(w, g["weights"][n - 1, :, :n]) < 1e-13
 
 
-def test_rys_fp32_tables_close():
+@pytest.mark.parametrize("n", range(1, 10))
+def test_rys_fp32_tables_close(n):
+    # FP32 power-form tables for every root count, T on both sides of tmax
     g = load_golden("rys.npz")
-    r, w = E.rys_roots(g["T"], 3, fp32=True)
-    assert _maxabs(r, g["roots"][2, :, :3]) < 1e-5
-    assert _maxabs(w, g["weights"][2, :, :3]) < 1e-5
+    r, w = E.rys_roots(g["T"], n, fp32=True)
+    er, ew = _maxabs(r, g["roots"][n - 1, :, :n]), _maxabs(w, g["weights"][n - 1, :, :n])
+    print(f"PIN rys_fp32_table N={n} abs_root={er:.2e} abs_weight={ew:.2e} T_max={g['T'].max():.1f}")
+    assert er < 2e-6 and ew < 2e-6
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_rys_fp32_interval_polynomials(n):
+    # the mixed-precision kernels' shared-memory polynomials (N <= 3)
+    g = load_golden("rys.npz")
+    r, w = E.rys_roots(g["T"], n, path="fp32_interval")
+    er, ew = _maxabs(r, g["roots"][n - 1, :, :n]), _maxabs(w, g["weights"][n - 1, :, :n])
+    print(f"PIN rys_fp32_interval N={n} abs_root={er:.2e} abs_weight={ew:.2e}")
+    assert er < 5e-7 and ew < 5e-7
+
+
+@pytest.mark.parametrize("n", [1, 2])
+def test_rys_fp64_boys_closed_forms(n):
+    # the FP64 N <= 2 kernels' closed forms from Boys values, against the
+    # reference's roots (its own 0.01-grid interpolant carries ~1e-13)
+    g = load_golden("rys.npz")
+    r, w = E.rys_roots(g["T"], n, path="fp64_boys")
+    er = _maxabs(r, g["roots"][n - 1, :, :n])
+    ew = _maxabs(w, g["weights"][n - 1, :, :n])
+    print(f"PIN rys_fp64_boys N={n} abs_root={er:.2e} abs_weight={ew:.2e}")
+    assert er < 1e-13 and ew < 1e-13
 
 
 def _check_blocks(ctx, g, tol):

@@ -40,15 +40,42 @@ def test_noalloc_blocks_match_allocating_entry_point_twice():
     expected = np.concatenate([b.ravel() for b in ctx.eri_blocks(quartets)])
 
     lib = N.lib()
-    for _ in range(2):
-        d_out = torch.full((total,), float("nan"), dtype=torch.float64, device="cuda")
-        torch.cuda.synchronize()
+    outs = [torch.full((total,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    free = []
+    for d_out in outs:
+        free.append(torch.cuda.mem_get_info()[0])
         rc = lib.tlno_gpu_eri_blocks_noalloc(ctx.h, len(quartets), quartets.ctypes.data, offsets.ctypes.data,
                                              C.c_void_p(d_out.data_ptr()))
         N.check(rc)
+        free.append(torch.cuda.mem_get_info()[0])
         got = d_out.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert float(np.max(np.abs(got - expected))) < 1e-12
+    # the calls take no device memory: free memory is the same before and
+    # after each of them
+    assert free[0] == free[1] and free[2] == free[3], free
+    ctx.close()
+
+
+def test_noalloc_blocks_match_the_reference_fixture():
+    """The entry point's blocks against the reference's own blocks (the
+    golden fixture written from the compiled reference)."""
+    import torch
+    from tests.conftest import load_golden
+
+    g = load_golden("cfg1.npz")
+    ctx = E.Context(M.cfg1())
+    q = np.ascontiguousarray(g["quartets"], dtype=np.int32)
+    offsets = np.ascontiguousarray(g["eri_off"][:-1], dtype=np.int64)
+    total = int(g["eri_off"][-1])
+    d_out = torch.zeros(total, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    N.check(N.lib().tlno_gpu_eri_blocks_noalloc(ctx.h, len(q), q.ctypes.data, offsets.ctypes.data,
+                                                C.c_void_p(d_out.data_ptr())))
+    err = float(np.max(np.abs(d_out.cpu().numpy() - g["eri"][:total])))
+    print(f"PIN noalloc_vs_reference_blocks max_abs={err:.2e}")
+    assert err < 1e-12
     ctx.close()
 
 
