@@ -340,6 +340,8 @@ def run_batch(args):
     opts = E.ScreeningOptions(integral_threshold=1e-12, mixed_threshold=args.mixed_threshold)
     ctxs = [E.Context(m, device=local) for m in mols]
     batch = E.Batch(ctxs, opts)
+    if args.streams > 1:
+        batch.set_tuning(streams=args.streams)
     prof = batch.profile()
     Ds = [torch.tensor(MOL.random_density(m.n_sph, max(1, m.n_sph // 5), seed=100 + i)) for i, m in enumerate(mols)]
     D = torch.cat([d.ravel() for d in Ds]).to(dev)
@@ -384,6 +386,7 @@ def run_batch(args):
            "data": "synthetic",
            "config": {"workload": "cfg3", "description": "256 molecules of 3-30 atoms in one batch, Schwarz 1e-12",
                       "molecules": len(mols), "functions_total": prof["M"], "quartets_per_build": q,
+                      "streams": args.streams,
                       "mixed_threshold": args.mixed_threshold},
            "fp64": {"value": q * args.steps / t64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps},
            "one_context_per_molecule_fp64_ms": 1e3 * seq,
@@ -409,6 +412,8 @@ def run_native(args):
     M = mol.n_sph
     ctx = E.Context(mol, device=local).plan(E.ScreeningOptions(integral_threshold=tau,
                                                                mixed_threshold=args.mixed_threshold))
+    if args.streams > 1:
+        ctx.set_tuning(streams=args.streams)
     prof = ctx.profile()
     quartets = prof["quartets"]
 
@@ -447,12 +452,14 @@ def run_native(args):
     # FP64 sequence first (also the accuracy reference for the last density)
     ms64 = timed_sequence(False)
     J64, K64 = J.clone(), K.clone()
-    # split threshold of the mixed path: autotuned on the last density
-    # against its FP64 build, 3x inside the accuracy targets
+    # split threshold of the mixed path, per class: autotuned on the last
+    # density, the summed per-class errors 3x inside the accuracy targets
     tune = None
     if not args.no_autotune:
-        from origo_tlno_b200.autotune import tune_mixed_threshold
-        tune = tune_mixed_threshold(ctx, Ds[-1], tol_energy=TOL_ENERGY / 3, tol_jk=TOL_JK / 3, reference=(J64, K64))
+        from origo_tlno_b200.autotune import tune_classes
+        t0 = time.time()
+        tune = tune_classes(ctx, Ds[-1], tol_energy=TOL_ENERGY / 3, tol_jk=TOL_JK / 3)
+        tune["tuning_s"] = time.time() - t0
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -540,9 +547,11 @@ def run_native(args):
         "config": {"workload": args.config, "description": wdesc, "M": M, "quartets_per_build": quartets,
                    "primitive_quartets_per_build": prof["primitive_quartets"],
                    "flops_per_build_model": prof["flops"], "parallelism": f"replicas{ws}",
+                   "streams": args.streams,
                    "l2": "inputs larger than L2 (D, J, K are M*M*8 bytes each)" if M * M * 8 > 126e6 else
                          "inputs smaller than L2",
-                   "mixed_threshold": tune["threshold"] if tune else args.mixed_threshold, "schwarz": tau},
+                   "mixed_threshold": "per class (mixed_autotune)" if tune else args.mixed_threshold,
+                   "schwarz": tau},
         "mixed_autotune": tune,
         "jk_builds_per_s": ws * steps / tmx,
         "fp64": {"value": value64, "unit": UNIT, "jk_builds_per_s": ws * steps / t64,
@@ -580,6 +589,8 @@ def main():
     ap.add_argument("--config", default="cfg4")
     ap.add_argument("--mixed-threshold", type=float, default=1e-9)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--streams", type=int, default=1,
+                    help="streams the class launches of a build spread over (1..4)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the incremental, ERI-stream and one-electron legs")
     ap.add_argument("--no-autotune", action="store_true",

@@ -312,19 +312,38 @@ void* tlno_gpu_batch_stream(tlno_gpu_batch* b);
 /* Tuning of the kernel schedule: generic-kernel ket tile, generic warps
  * per CTA (0 = from the shared-memory budget), persistent grid multiplier
  * (the compile-time kernels size their grid from the occupancy calculator,
- * capped by grid_mult x SMs); and a per-class-combination generic
- * override. */
+ * capped by grid_mult x SMs), and streams (1..4): the class launches of a
+ * build spread over that many streams (parallel branches of a captured
+ * graph), so that the tail of one class overlaps the next; 1 keeps them in
+ * order on the context's stream.  A per-class-combination generic override
+ * is set separately. */
 typedef struct {
     int generic_bk;
     int generic_warps;
     int grid_mult;
+    int streams;
 } tlno_gpu_tuning;
 int tlno_gpu_set_tuning(tlno_gpu_context* ctx, const tlno_gpu_tuning* t);
+/* The same for a batch (its schedule keeps the ket tile of its plan). */
+int tlno_gpu_batch_set_tuning(tlno_gpu_batch* b, const tlno_gpu_tuning* t);
 int tlno_gpu_set_combo_generic(tlno_gpu_context* ctx, int combo_id, int force_generic);
 /* Per class-combination statistics of the current plan: for i < n, writes
  * (X, Y, la, lb, lc, ld, fast, n_tiles) into ints[8*i] and
  * (quartets, prim_quartets, flops) into dbl[3*i]; returns the count. */
 int tlno_gpu_plan_combos(const tlno_gpu_context* ctx, int max_n, int* ints, double* dbl);
+/* Per-class tuning of the current plan (the per-class autotuner's knobs;
+ * no reference counterpart): the split threshold of class combination
+ * combo_index is mixed_threshold x mixed_scale (> 0), and its compile-time
+ * kernel takes tile_chunk tiles of 32 ket pairs per fetch of its dynamic
+ * schedule (1..64; 0 = the kernel's default of 4).  Re-planning resets
+ * them.  A captured J/K graph keeps the values of its capture. */
+int tlno_gpu_set_class_tuning(tlno_gpu_context* ctx, int combo_index, double mixed_scale, int tile_chunk);
+/* J and K contributions of one class combination alone (device buffers,
+ * J and K zeroed first, not symmetrised), FP64 or with TLNO_GPU_MIXED the
+ * split of the class's tuning; *ms (may be null) receives the device time of
+ * the class kernels.  For the per-class autotuner's error and time model. */
+int tlno_gpu_class_jk(tlno_gpu_context* ctx, int combo_index, const double* d_density, double* d_J,
+                      double* d_K, int flags, double* ms);
 /* Time one class combination alone (ms per launch, CUDA events) for the
  * autotuner; runs on the context's stream with its device buffers.
  * mode bits: 1 = FP32 evaluation, 2 = skip the J digestion, 4 = skip the K

@@ -64,7 +64,7 @@ class IncrementalInfo(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("generic_bk", C.c_int), ("generic_warps", C.c_int), ("grid_mult", C.c_int)]
+    _fields_ = [("generic_bk", C.c_int), ("generic_warps", C.c_int), ("grid_mult", C.c_int), ("streams", C.c_int)]
 
 
 _lib = None
@@ -132,6 +132,9 @@ def lib() -> C.CDLL:
         "tlno_gpu_set_combo_generic": (C.c_int, [_vp, C.c_int, C.c_int]),
         "tlno_gpu_plan_combos": (C.c_int, [_vp, C.c_int, _vp, _vp]),
         "tlno_gpu_time_combo": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _dp]),
+        "tlno_gpu_set_class_tuning": (C.c_int, [_vp, C.c_int, C.c_double, C.c_int]),
+        "tlno_gpu_batch_set_tuning": (C.c_int, [_vp, C.POINTER(Tuning)]),
+        "tlno_gpu_class_jk": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, _dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -171,4 +174,5 @@ EXPORTED = [
     "tlno_gpu_batch_profile", "tlno_gpu_batch_jk", "tlno_gpu_batch_graph_capture",
     "tlno_gpu_batch_graph_launch", "tlno_gpu_batch_synchronize", "tlno_gpu_batch_stream",
     "tlno_gpu_set_tuning", "tlno_gpu_set_combo_generic", "tlno_gpu_plan_combos", "tlno_gpu_time_combo",
+    "tlno_gpu_set_class_tuning", "tlno_gpu_class_jk", "tlno_gpu_batch_set_tuning",
 ]

@@ -124,8 +124,30 @@ BuildSpec spec_from(const tlno_gpu_screening& o, bool want_j, bool want_k, bool 
 
 // Enqueues one J/K build on stream s over device buffers (the density tables
 // of a density-screened build must be allocated before: ensure_density_tables).
+void StreamFan::ensure(int n_aux) {
+    TLNO_CUDA(cudaGetDevice(&device));
+    while (static_cast<int>(aux.size()) < n_aux) {
+        cudaStream_t st = nullptr;
+        TLNO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        aux.push_back(st);
+    }
+    while (static_cast<int>(ev.size()) < n_aux + 1) {
+        cudaEvent_t e = nullptr;
+        TLNO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev.push_back(e);
+    }
+}
+
+StreamFan::~StreamFan() {
+    if (aux.empty() && ev.empty()) return;
+    cudaSetDevice(device);
+    for (cudaStream_t st : aux) cudaStreamDestroy(st);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+}
+
 void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const double* dD, double* dJ,
-                double* dK, long long total, int M_single, double* d_dmax, float* dD32, cudaStream_t s) {
+                double* dK, long long total, int M_single, double* d_dmax, float* dD32, cudaStream_t s,
+                StreamFan* fan) {
     const bool want_j = spec.want_j, want_k = spec.want_k, mixed = spec.mixed;
     TLNO_CUDA(cudaMemsetAsync(dJ, 0, sizeof(double) * total, s));
     TLNO_CUDA(cudaMemsetAsync(dK, 0, sizeof(double) * total, s));
@@ -152,8 +174,34 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const d
     int sms = 0, devid = 0;
     TLNO_CUDA(cudaGetDevice(&devid));
     TLNO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devid));
+    // Class launches over `nst` streams: fork after the shared prologue
+    // (zeroing, max|D|, density tables), each class on the stream with the
+    // least flops so far (largest classes first), join before the
+    // symmetrisation.  J and K take FP64 atomics, so the order is free.
+    const int nst = (fan && tune.streams > 1) ? std::min(tune.streams, 4) : 1;
+    std::vector<cudaStream_t> st(1, s);
+    std::vector<int> stream_of(plan.combos.size(), 0);
+    if (nst > 1) {
+        fan->ensure(nst - 1);
+        TLNO_CUDA(cudaEventRecord(fan->ev[0], s));
+        for (int k = 0; k < nst - 1; ++k) {
+            TLNO_CUDA(cudaStreamWaitEvent(fan->aux[k], fan->ev[0], 0));
+            st.push_back(fan->aux[k]);
+        }
+        std::vector<std::size_t> order(plan.combos.size());
+        for (std::size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](std::size_t a, std::size_t b) { return plan.combos[a].flops > plan.combos[b].flops; });
+        std::vector<double> load(nst, 0.0);
+        for (std::size_t i : order) {
+            const int k = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+            stream_of[i] = k;
+            load[k] += plan.combos[i].flops;
+        }
+    }
     for (std::size_t ci = 0; ci < plan.combos.size(); ++ci) {
         ComboSchedule& cs = plan.combos[ci];
+        cudaStream_t cs_stream = st[stream_of[ci]];
         dev::ClassLaunch cl{};
         cl.la = cs.la; cl.lb = cs.lb; cl.lc = cs.lc; cl.ld = cs.ld;
         cl.same = (cs.X == cs.Y);
@@ -166,7 +214,8 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const d
         cl.tile_begin = 0;
         cl.tile_end = cs.n_tiles;
         cl.tau = plan.tau;
-        cl.tau_mix = spec.mixed_threshold;
+        cl.tau_mix = spec.mixed_threshold * cs.mix_scale;
+        cl.chunk = cs.chunk;
         cl.den = den;
         cl.fs_thr2 = spec.fs_thr2;
         cl.M_shells = plan.mol_ns.empty() ? 0 : plan.mol_ns[0];
@@ -185,10 +234,16 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const d
             cl.counter = plan.d_counters.as<int>() + 2 * ci + pass;
             const bool fp32 = mixed && pass == 1;
             if (cs.fast) {
-                launch_eri_jk_fast(pv, cl, fp32, grid, s);
+                launch_eri_jk_fast(pv, cl, fp32, grid, cs_stream);
             } else {
-                launch_eri_jk_generic(pv, cl, fp32, tune.generic_warps, grid, s);
+                launch_eri_jk_generic(pv, cl, fp32, tune.generic_warps, grid, cs_stream);
             }
+        }
+    }
+    if (nst > 1) {
+        for (int k = 0; k < nst - 1; ++k) {
+            TLNO_CUDA(cudaEventRecord(fan->ev[k + 1], fan->aux[k]));
+            TLNO_CUDA(cudaStreamWaitEvent(s, fan->ev[k + 1], 0));
         }
     }
     if (plan.n_mol > 1) {
@@ -341,7 +396,7 @@ void run_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, 
         const bool pj = den ? out_j : (out_j || want_g);
         const bool pk = den ? out_k : (out_k || want_g);
         enqueue_jk(*ctx->plan, ctx->tune, spec_from(eo, pj, pk, mixed, false), dD, dJ, dK, n, M,
-                   ctx->w.dmax.as<double>(), d32, s);
+                   ctx->w.dmax.as<double>(), d32, s, &ctx->fan);
         if (!dev_ptrs) {
             if (out_j) TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
             if (out_k) TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -354,7 +409,7 @@ void run_jk(tlno_gpu_context* ctx, const double* density, double* J, double* K, 
             gJ = ctx->w.J.as<double>();
             gK = ctx->w.K.as<double>();
             enqueue_jk(*ctx->plan, ctx->tune, spec_from(eo, true, true, mixed, true), dD, gJ, gK, n, M,
-                       ctx->w.dmax.as<double>(), d32, s);
+                       ctx->w.dmax.as<double>(), d32, s, &ctx->fan);
         }
         double* dG = G;
         if (!dev_ptrs) {
@@ -782,7 +837,7 @@ int tlno_gpu_jk_graph_capture(tlno_gpu_context* ctx, const double* d_density, do
         TLNO_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         try {
             enqueue_jk(*ctx->plan, ctx->tune, spec, d_density, d_J, d_K, n, M, ctx->w.dmax.as<double>(), d32,
-                       ctx->stream);
+                       ctx->stream, &ctx->fan);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(ctx->stream, &g);
@@ -816,8 +871,9 @@ int tlno_gpu_set_tuning(tlno_gpu_context* ctx, const tlno_gpu_tuning* t) {
     return guarded([&] {
         if (!ctx || !t) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
         if (t->generic_bk < 1 || t->generic_bk > 4096 || t->generic_warps < 0 || t->generic_warps > 8 ||
-            t->grid_mult < 1 || t->grid_mult > 64)
+            t->grid_mult < 1 || t->grid_mult > 64 || t->streams < 1 || t->streams > 4)
             throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: tuning value out of range");
+        ctx->tune.streams = t->streams;
         ctx->tune.generic_bk = t->generic_bk;
         ctx->tune.generic_warps = t->generic_warps;
         ctx->tune.grid_mult = t->grid_mult;
@@ -874,6 +930,7 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int re
         cl.tile_begin = 0;
         cl.tile_end = cs.n_tiles;
         cl.tau = plan.tau;
+        cl.chunk = cs.chunk;
         cl.dens = ctx->w.D.as<double>();
         ctx->w.D32.alloc(sizeof(float) * n);
         cl.dens32 = ctx->w.D32.as<float>();
@@ -905,6 +962,88 @@ int tlno_gpu_time_combo(tlno_gpu_context* ctx, int combo_index, int mode, int re
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         *ms = t / std::max(reps, 1);
+    });
+}
+
+int tlno_gpu_set_class_tuning(tlno_gpu_context* ctx, int combo_index, double mixed_scale, int tile_chunk) {
+    return guarded([&] {
+        if (!ctx || !ctx->plan) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan");
+        if (combo_index < 0 || combo_index >= static_cast<int>(ctx->plan->combos.size()))
+            throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: combo index out of range");
+        if (!finite_bits(mixed_scale) || !(mixed_scale > 0.0) || tile_chunk < 0 || tile_chunk > 64)
+            throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: class tuning value out of range");
+        ctx->plan->combos[combo_index].mix_scale = mixed_scale;
+        ctx->plan->combos[combo_index].chunk = tile_chunk;
+    });
+}
+
+int tlno_gpu_class_jk(tlno_gpu_context* ctx, int combo_index, const double* d_density, double* d_J, double* d_K,
+                      int flags, double* ms) {
+    return guarded([&] {
+        if (!ctx || !ctx->plan || !d_density || !d_J || !d_K) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan");
+        Plan2e& plan = *ctx->plan;
+        if (combo_index < 0 || combo_index >= static_cast<int>(plan.combos.size()))
+            throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: combo index out of range");
+        TLNO_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t s = ctx->stream;
+        const int M = ctx->basis.n_sph;
+        const long long n = static_cast<long long>(M) * M;
+        ensure_work(ctx->w, 1);
+        const bool mixed = flags & TLNO_GPU_MIXED;
+        float* d32 = nullptr;
+        if (mixed) {
+            ctx->w.D32.alloc(sizeof(float) * n);
+            d32 = ctx->w.D32.as<float>();
+        }
+        TLNO_CUDA(cudaMemsetAsync(d_J, 0, sizeof(double) * n, s));
+        TLNO_CUDA(cudaMemsetAsync(d_K, 0, sizeof(double) * n, s));
+        TLNO_CUDA(cudaMemsetAsync(plan.d_counters.ptr, 0, sizeof(int) * 2 * plan.combos.size(), s));
+        if (mixed) launch_absmax_f32(d_density, n, ctx->w.dmax.as<double>(), d32, s);
+        ComboSchedule& cs = plan.combos[combo_index];
+        dev::ClassLaunch cl{};
+        cl.la = cs.la; cl.lb = cs.lb; cl.lc = cs.lc; cl.ld = cs.ld;
+        cl.same = (cs.X == cs.Y);
+        cl.bb = cs.bb; cl.bk = cs.bk;
+        cl.blocks = cs.d_blocks.as<dev::BlockDesc>();
+        cl.bra_list = cs.d_bra_list.as<int>();
+        cl.tile_prefix = cs.d_prefix.as<int>();
+        cl.n_blocks = static_cast<int>(cs.blocks.size());
+        cl.tile_begin = 0;
+        cl.tile_end = cs.n_tiles;
+        cl.tau = plan.tau;
+        cl.tau_mix = ctx->screening.mixed_threshold * cs.mix_scale;
+        cl.chunk = cs.chunk;
+        cl.dmax = ctx->w.dmax.as<double>();
+        cl.dens = d_density;
+        cl.dens32 = d32;
+        cl.J = d_J;
+        cl.K = d_K;
+        cl.M = M;
+        cl.want_j = 1;
+        cl.want_k = 1;
+        int sms = 0;
+        TLNO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        const dev::PlanView pv = plan.view();
+        cudaEvent_t e0, e1;
+        TLNO_CUDA(cudaEventCreate(&e0));
+        TLNO_CUDA(cudaEventCreate(&e1));
+        TLNO_CUDA(cudaEventRecord(e0, s));
+        for (int pass = 0; pass < (mixed ? 2 : 1); ++pass) {
+            cl.prec_mode = mixed ? pass + 1 : 0;
+            cl.counter = plan.d_counters.as<int>() + 2 * combo_index + pass;
+            const bool fp32 = mixed && pass == 1;
+            if (cs.fast)
+                launch_eri_jk_fast(pv, cl, fp32, sms * ctx->tune.grid_mult, s);
+            else
+                launch_eri_jk_generic(pv, cl, fp32, ctx->tune.generic_warps, sms * ctx->tune.grid_mult, s);
+        }
+        TLNO_CUDA(cudaEventRecord(e1, s));
+        TLNO_CUDA(cudaEventSynchronize(e1));
+        float t = 0.f;
+        TLNO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (ms) *ms = t;
     });
 }
 
@@ -943,6 +1082,18 @@ int tlno_gpu_batch_create(int n_mol, tlno_gpu_context* const* ctxs, const tlno_g
 }
 
 void tlno_gpu_batch_destroy(tlno_gpu_batch* b) { delete b; }
+
+int tlno_gpu_batch_set_tuning(tlno_gpu_batch* b, const tlno_gpu_tuning* t) {
+    return guarded([&] {
+        if (!b || !t) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: null argument");
+        if (t->generic_bk < 1 || t->generic_bk > 4096 || t->generic_warps < 0 || t->generic_warps > 8 ||
+            t->grid_mult < 1 || t->grid_mult > 64 || t->streams < 1 || t->streams > 4)
+            throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: tuning value out of range");
+        b->tune.generic_warps = t->generic_warps;
+        b->tune.grid_mult = t->grid_mult;
+        b->tune.streams = t->streams;
+    });
+}
 
 long long tlno_gpu_batch_total_elements(const tlno_gpu_batch* b) { return b ? b->total : -1; }
 
@@ -993,7 +1144,7 @@ int tlno_gpu_batch_jk(tlno_gpu_batch* b, const double* density, double* J, doubl
         validate_build_combination(b->screening);
         if (b->screening.density_threshold > 0.0) ensure_density_tables(b->plan);
         enqueue_jk(b->plan, b->tune, spec_from(b->screening, true, true, flags & TLNO_GPU_MIXED, false), dD, dJ, dK,
-                   b->total, 0, b->w.dmax.as<double>(), d32, s);
+                   b->total, 0, b->w.dmax.as<double>(), d32, s, &b->fan);
         if (!dev_ptrs) {
             TLNO_CUDA(cudaMemcpyAsync(J, dJ, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
             TLNO_CUDA(cudaMemcpyAsync(K, dK, sizeof(double) * b->total, cudaMemcpyDeviceToHost, s));
@@ -1020,7 +1171,7 @@ int tlno_gpu_batch_graph_capture(tlno_gpu_batch* b, const double* d_density, dou
         TLNO_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         try {
             enqueue_jk(b->plan, b->tune, spec, d_density, d_J, d_K, b->total, 0, b->w.dmax.as<double>(), d32,
-                       b->stream);
+                       b->stream, &b->fan);
         } catch (...) {
             cudaGraph_t g = nullptr;
             cudaStreamEndCapture(b->stream, &g);

@@ -19,6 +19,16 @@ void set_last_error(const std::string& message);
 // of the fixed scratch of tlno_gpu_eri_blocks_noalloc.
 void noalloc_prepare(int device);
 
+// Auxiliary streams and fork/join events of a build whose class launches
+// run on several streams (created on first use, destroyed with the owner).
+struct StreamFan {
+    int device = 0;
+    std::vector<cudaStream_t> aux;
+    std::vector<cudaEvent_t> ev;
+    void ensure(int n_aux);
+    ~StreamFan();
+};
+
 struct JkWork {
     DeviceBuffer D, J, K, G, dmax, status;
     DeviceBuffer D32;  // FP32 copy of the density for the FP32 kernels (mixed builds)
@@ -38,6 +48,7 @@ struct tlno_gpu_context {
     tlno_gpu::DeviceBuffer d_shell_xyz, d_shell_L, d_shell_nprim, d_shell_prim, d_shell_sph, d_exps, d_crad;
     tlno_gpu::DeviceBuffer d_comp_coef, d_comp_off;
     tlno_gpu::JkWork w;
+    tlno_gpu::StreamFan fan;
     tlno_gpu::DeviceBuffer d_S, d_T, d_V;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -58,6 +69,7 @@ struct tlno_gpu_batch {
     tlno_gpu_screening screening{};
     tlno_gpu::Tuning tune;
     tlno_gpu::JkWork w;
+    tlno_gpu::StreamFan fan;
     long long total = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;

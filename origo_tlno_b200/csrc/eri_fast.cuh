@@ -77,7 +77,7 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
 }
 
 constexpr int kMaxAccPerSlice = 64;
-constexpr int kTileChunk = 4;  // tiles per dynamic-schedule fetch
+constexpr int kTileChunk = 4;  // default tiles per dynamic-schedule fetch
 constexpr int kBraGroup = 8;   // bras per block of the light classes
 constexpr int kMaxCarried = 24;
 
@@ -414,7 +414,9 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     const int ntiles = cl.tile_end - cl.tile_begin;
     double csum = 0.0;  // ERI checksum stream: this thread's share
 
-    // Dynamic schedule: every warp group takes kTileChunk consecutive tiles
+    // tiles per fetch (per-class tuning; 0 = the default)
+    const int chunk = cl.chunk > 0 ? cl.chunk : kTileChunk;
+    // Dynamic schedule: every warp group takes `chunk` consecutive tiles
     // (one bra pair x 32 kets each) from the launch counter, so all groups
     // work inside one moving window of the schedule and the density, J and
     // K rows of the bras in flight stay in L2.  The first tile's block comes
@@ -422,16 +424,16 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
     for (;;) {
         int c0;
         if constexpr (S::TPQ == 1) {
-            c0 = (lane == 0) ? atomicAdd(cl.counter, kTileChunk) : 0;
+            c0 = (lane == 0) ? atomicAdd(cl.counter, chunk) : 0;
             c0 = __shfl_sync(0xffffffffu, c0, 0);
         } else {
-            if (g == 0 && lane == 0) s_chunk[grp] = atomicAdd(cl.counter, kTileChunk);
+            if (g == 0 && lane == 0) s_chunk[grp] = atomicAdd(cl.counter, chunk);
             group_sync(bar_id, bar_n);
             c0 = s_chunk[grp];
             group_sync(bar_id, bar_n);
         }
         if (c0 >= ntiles) break;
-        const int c1 = min(c0 + kTileChunk, ntiles);
+        const int c1 = min(c0 + chunk, ntiles);
         int b = find_block(cl.tile_prefix, cl.n_blocks, cl.tile_begin + c0);
         int next = __ldg(cl.tile_prefix + b + 1);
     for (int tile = cl.tile_begin + c0; tile < cl.tile_begin + c1; ++tile) {

@@ -47,7 +47,8 @@ BuildSpec spec_from(const tlno_gpu_screening& o, bool want_j, bool want_k, bool 
 // class kernels, the final symmetrisation.  A density-screened build needs
 // ensure_density_tables(plan) first.
 void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const double* dD, double* dJ,
-                double* dK, long long total, int M_single, double* d_dmax, float* dD32, cudaStream_t s);
+                double* dK, long long total, int M_single, double* d_dmax, float* dD32, cudaStream_t s,
+                StreamFan* fan = nullptr);
 
 // Two-electron plan of a context's basis for the shell-level screen of o.
 std::unique_ptr<Plan2e> make_plan(const tlno_gpu_context* ctx, const tlno_gpu_screening& o);

@@ -81,6 +81,7 @@ struct ClassLaunch {
     int n_blocks;
     int tile_begin, tile_end;     // tile range of this launch
     int* counter;                 // dynamic-schedule counter, zero at launch (compile-time kernels)
+    int chunk;                    // tiles per counter fetch (0 = kernel default)
     double tau;                   // Schwarz threshold
     // Precision split: mode 0 = every quartet; 1 = quartets with
     // Q_ab Q_cd max|D| >= tau_mix only (FP64 part); 2 = the complement.

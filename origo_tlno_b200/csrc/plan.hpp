@@ -15,6 +15,7 @@ struct Tuning {
     int generic_bk = 64;    // ket pairs per tile of the warp-per-quartet kernel
     int generic_warps = 0;  // 0 = from shared-memory budget
     int grid_mult = 8;      // CTAs per SM for persistent launches
+    int streams = 1;        // streams the class launches of a build spread over
     std::array<int, 256> force_generic{};  // per class combo: 1 = never use the fast kernel
 };
 
@@ -23,6 +24,10 @@ struct ComboSchedule {
     int la = 0, lb = 0, lc = 0, ld = 0;
     bool fast = false;
     int bb = 1, bk = 16;
+    // per-class tuning: split threshold multiplier of the mixed path and
+    // tiles per dynamic-schedule fetch (0 = kernel default)
+    double mix_scale = 1.0;
+    int chunk = 0;
     std::vector<dev::BlockDesc> blocks;
     std::vector<int> prefix;
     std::vector<int> bra_list;

@@ -223,8 +223,8 @@ class Context:
         N.check(N.lib().tlno_gpu_set_onee_thresholds(self.h, decay_eps, nuclear_eps))
 
     # -- tuning ---------------------------------------------------------
-    def set_tuning(self, generic_bk=64, generic_warps=0, grid_mult=8):
-        t = N.Tuning(generic_bk, generic_warps, grid_mult)
+    def set_tuning(self, generic_bk=64, generic_warps=0, grid_mult=8, streams=1):
+        t = N.Tuning(generic_bk, generic_warps, grid_mult, streams)
         N.check(N.lib().tlno_gpu_set_tuning(self.h, C.byref(t)))
 
     def set_combo_generic(self, combo_id: int, force: bool):
@@ -281,6 +281,10 @@ class Batch:
         p = N.Profile()
         N.check(N.lib().tlno_gpu_batch_profile(self.h, C.byref(p)))
         return {f: getattr(p, f) for f, _ in N.Profile._fields_}
+
+    def set_tuning(self, generic_bk=64, generic_warps=0, grid_mult=8, streams=1):
+        t = N.Tuning(generic_bk, generic_warps, grid_mult, streams)
+        N.check(N.lib().tlno_gpu_batch_set_tuning(self.h, C.byref(t)))
 
     def jk(self, densities, mixed=False):
         D = np.concatenate([_f64(d).ravel() for d in densities])

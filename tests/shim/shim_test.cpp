@@ -8,6 +8,8 @@
 // tests/test_gpu_shim.py.
 //
 // Shell file: n_shells, then per shell "x y z L nprim e_1..e_n c_1..c_n".
+#include <omp.h>
+
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -29,7 +31,24 @@ double maxdiff(const std::vector<double>& a, const std::vector<double>& b) {
 
 }  // namespace
 
+int run(int argc, char** argv);
+
 int main(int argc, char** argv) {
+    // the reference's G and K endpoints refuse more than one OpenMP thread
+    // (rys_engine.ipp:16853-16857)
+    omp_set_num_threads(1);
+    try {
+        return run(argc, argv);
+    } catch (const std::exception& e) {
+        std::string msg = e.what();
+        for (char& c : msg)
+            if (c == '"') c = '\'';
+        std::printf("{\"error\": \"%s\"}\n", msg.c_str());
+        return 3;
+    }
+}
+
+int run(int argc, char** argv) {
     if (argc < 2) {
         std::fprintf(stderr, "usage: shim_test SHELL_FILE [schwarz] [density_threshold]\n");
         return 2;

@@ -38,8 +38,10 @@ def test_cpp_shim_matches_reference(name, tmp_path):
     tau = "1e-12" if name == "cfg1" else "1e-11"
     r = subprocess.run([SHIM, str(path), tau, "1e-10"], capture_output=True, text=True, timeout=600)
     print(r.stdout, r.stderr)
-    res = json.loads(r.stdout.strip().splitlines()[-1])
-    assert r.returncode == 0, res
+    lines = r.stdout.strip().splitlines()
+    assert lines, r.stderr
+    res = json.loads(lines[-1])
+    assert r.returncode == 0 and "error" not in res, res
     assert res["M"] == mol.n_sph
     assert res["incremental_status_match"] and res["same_error_text"]
     assert max(res["J"], res["K"], res["G"], res["G_density_screened"], res["incremental_G"]) < 1e-12
