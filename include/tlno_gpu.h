@@ -270,8 +270,7 @@ int tlno_gpu_boys(int device, int n, int maxn, const double* x, double* out);
  * (rys_engine.ipp:3823-3838).  fp32 selects the evaluation path of the
  * kernels: 0 = FP64 tables (the reference's 0.01-grid interpolant),
  * 1 = FP32 tables, 2 = the FP32 interval polynomials of the mixed-precision
- * kernels (nroots <= 3), 3 = the FP64 closed forms from Boys values of the
- * N <= 2 kernels (nroots <= 2). */
+ * kernels (nroots <= 3). */
 int tlno_gpu_rys(int device, int n, int nroots, const double* T, double* roots, double* weights,
                  int fp32);
 

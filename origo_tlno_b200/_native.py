@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libtlno_gpu.so")
+# TLNO_GPU_LIB selects another build of the same library (same C ABI)
+LIB_PATH = os.environ.get("TLNO_GPU_LIB") or os.path.join(_HERE, "_lib", "libtlno_gpu.so")
 
 OK = 0
 E_INVALID = -1

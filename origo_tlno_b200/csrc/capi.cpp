@@ -787,7 +787,7 @@ int tlno_gpu_boys(int device, int n, int maxn, const double* x, double* out) {
 int tlno_gpu_rys(int device, int n, int nroots, const double* T, double* roots, double* weights, int fp32) {
     return guarded([&] {
         if (n < 0 || nroots < 1 || nroots > kRysMaxN) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: nroots must be 1..9");
-        if (fp32 < 0 || fp32 > 3 || (fp32 == 2 && nroots > 3) || (fp32 == 3 && nroots > 2))
+        if (fp32 < 0 || fp32 > 2 || (fp32 == 2 && nroots > 3))
             throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: Rys evaluation mode out of range for nroots");
         for (int i = 0; i < n; ++i)
             if (!finite_bits(T[i]) || T[i] < 0.0) throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: Rys argument must be finite and >= 0");

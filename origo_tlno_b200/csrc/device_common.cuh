@@ -31,14 +31,12 @@ struct DevTables {
     // (lowest power of u = 4T - k - 1/2 first); staged in shared memory.
     const float* rys32[4];
     int rys32_nint[4];
-    // FP64 Boys interval polynomials of F_{2N-1} for N = 1, 2: interval k of
-    // width 1/4 holds 10 coefficients (lowest power of u = 4T - k - 1/2
-    // first); staged in shared memory by the N <= 2 FP64 kernels.
-    const double* boys_iv[3];
-    int boys_iv_nint[3];
+    // The reference's raw 0.01-grid values for N = 1, one (root, weight)
+    // pair per grid row (46.5 KB), staged in shared memory by the FP64 N = 1
+    // kernels.
+    const double* rys_raw1;
+    int rys_raw1_rows;
 };
-constexpr int kBoysIvCoefDev = 10;
-constexpr int kBoysIvPerUnitDev = 4;
 constexpr int kRys32PerUnitDev = 4;
 constexpr int kRys32CoefDev = 6;
 
@@ -203,65 +201,32 @@ __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
     }
 }
 
-// FP64 roots and weights for N <= 2 from Boys values (the Rys quadrature
-// moments mu_k = F_k(T)): F_{2N-1} from the shared-memory interval
-// polynomials, F_{2N-2} .. F_0 by the downward recursion
-// F_{n-1} = (2T F_n + e^{-T}) / (2n - 1), then the Gauss rule of the moments
-// in closed form -- N = 1: t^2 = F_1 / F_0, w = F_0; N = 2: the eigenpairs of
-// the 2 x 2 Jacobi matrix of the monic recurrence (a0 = mu1/mu0,
-// b1 = (mu2 - a0 mu1)/mu0, a1 = (mu3 - a0 mu2)/(mu2 - a0 mu1) - a0), weights
-// mu0 b1 / (b1 + (t^2 - a0)^2).  Above tmax(N) the Hermite asymptotic form,
-// as rys_roots_all.
-template <int N>
-__device__ __forceinline__ void rys_roots_boys(double T, const double* __restrict__ table, double* root,
-                                               double* weight) {
-    static_assert(N == 1 || N == 2, "closed forms for one or two roots");
-    if (T >= c_tabs.tmax[N]) {
+// FP64 root and weight for N = 1 from the raw grid rows in shared memory
+// (f_k = (t^2, w) at T = 0.01 k), with the reference's 5-point
+// Newton-forward stencil over rows k..k+4 written out as it evaluates it
+// (rys_engine.ipp:3784-3812); the Hermite asymptotic form above tmax(1).
+__device__ __forceinline__ void rys_root1_raw(double T, const double2* __restrict__ rows, double& root,
+                                              double& weight) {
+    if (T >= c_tabs.tmax[1]) {
         const double inv = 1.0 / T;
-        const double sinv = sqrt(inv);
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-            root[i] = c_tabs.h2[N][i] * inv;
-            weight[i] = c_tabs.hw[N][i] * sinv;
-        }
+        root = c_tabs.h2[1][0] * inv;
+        weight = c_tabs.hw[1][0] * sqrt(inv);
         return;
     }
-    const double x = T * double(kBoysIvPerUnitDev);
-    const int k = static_cast<int>(x);
-    const double u = x - double(k) - 0.5;
-    const double2* rec = reinterpret_cast<const double2*>(table + k * kBoysIvCoefDev);
-    double c[kBoysIvCoefDev];
-#pragma unroll
-    for (int j = 0; j < kBoysIvCoefDev / 2; ++j) {
-        const double2 v = rec[j];
-        c[2 * j] = v.x;
-        c[2 * j + 1] = v.y;
-    }
-    double F[2 * N];
-    double v = c[kBoysIvCoefDev - 1];
-#pragma unroll
-    for (int j = kBoysIvCoefDev - 2; j >= 0; --j) v = fma(v, u, c[j]);
-    F[2 * N - 1] = v;
-    const double e = exp(-T), t2 = T + T;
-#pragma unroll
-    for (int n = 2 * N - 1; n >= 1; --n) F[n - 1] = fma(t2, F[n], e) * (1.0 / (2 * n - 1));
-    if constexpr (N == 1) {
-        root[0] = F[1] / F[0];
-        weight[0] = F[0];
-    } else {
-        const double a0 = F[1] / F[0];
-        const double s1 = fma(-a0, F[1], F[2]);
-        const double s2 = fma(-a0, F[2], F[3]);
-        const double a1 = s2 / s1 - a0;
-        const double b1 = s1 / F[0];
-        const double half = 0.5 * (a0 + a1), diff = 0.5 * (a0 - a1);
-        const double disc = sqrt(fma(diff, diff, b1));
-        root[0] = half - disc;
-        root[1] = half + disc;
-        const double d0 = root[0] - a0, d1 = root[1] - a0;
-        weight[0] = F[0] * b1 / fma(d0, d0, b1);
-        weight[1] = F[0] * b1 / fma(d1, d1, b1);
-    }
+    const double fi = T * 100.0;
+    const int k = static_cast<int>(fi);
+    const double t = fi - k;
+    const double tm1 = t - 1.0, tm2 = t - 2.0, tm3 = t - 3.0;
+    const double2 f0 = rows[k], f1 = rows[k + 1], f2 = rows[k + 2], f3 = rows[k + 3], f4 = rows[k + 4];
+    auto newton = [&](double a0, double a1, double a2, double a3, double a4) {
+        const double d1 = a1 - a0;
+        const double d2 = (a2 - 2.0 * a1 + a0) * 0.5;
+        const double d3 = (a3 - 3.0 * a2 + 3.0 * a1 - a0) * (1.0 / 6.0);
+        const double d4 = (a4 - 4.0 * a3 + 6.0 * a2 - 4.0 * a1 + a0) * (1.0 / 24.0);
+        return a0 + t * (d1 + tm1 * (d2 + tm2 * (d3 + tm3 * d4)));
+    };
+    root = newton(f0.x, f1.x, f2.x, f3.x, f4.x);
+    weight = newton(f0.y, f1.y, f2.y, f3.y, f4.y);
 }
 
 // FP32 roots and weights for N <= 3 from the shared-memory interval

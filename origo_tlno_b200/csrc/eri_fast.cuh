@@ -198,9 +198,9 @@ template <typename R, int LA, int LB, int LC, int LD, int G>
 __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
                                            double fs_thr2, const void* rtab_v, R* __restrict__ ks) {
     // shared-memory root tables: FP32 interval polynomials (FP32, N <= 3) or
-    // FP64 Boys interval polynomials (FP64, N <= 2)
+    // the raw N = 1 grid (FP64, N = 1)
     const float* rtab = static_cast<const float*>(rtab_v);
-    const double* rtab64 = static_cast<const double*>(rtab_v);
+    const double2* rtab64 = static_cast<const double2*>(rtab_v);
     using S = FastShape<LA, LB, LC, LD>;
     constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
     R acc[ROWS > 0 ? ROWS : 1][S::NCS];
@@ -276,9 +276,8 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
                         rt[r] = R(rd[r]);
                         wt[r] = R(wd[r]);
                     }
-                } else if constexpr (S::N <= 2) {
-                    // closed forms from Boys values, no table gather
-                    rys_roots_boys<S::N>(Targ, rtab64, rt, wt);
+                } else if constexpr (S::N == 1) {
+                    rys_root1_raw(Targ, rtab64, rt[0], wt[0]);
                 } else {
                     rys_roots_all<R, S::N>(Targ, rt, wt);
                 }
@@ -374,8 +373,13 @@ __device__ __forceinline__ bool group_any(bool pred, int id, int nthreads) {
     return r != 0;
 }
 
+// Unsliced classes are latency-bound on their gathers: the register cap of
+// 4 resident CTAs per SM (FP64) or 6 (FP32) buys more warps than it costs in
+// spills (measured on the six s/p classes of 200 waters: 589 -> 561 ms FP64,
+// 372 -> 364 ms FP32 summed).
 template <typename R, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
+__global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
+                                  FastShape<LA, LB, LC, LD>::TPQ == 1 ? (std::is_same<R, float>::value ? 6 : 4) : 1)
     eri_fast_jk_kernel(PlanView pv, ClassLaunch cl) {
     using S = FastShape<LA, LB, LC, LD>;
     extern __shared__ double fast_smem[];
@@ -401,12 +405,11 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
         for (int i = threadIdx.x; i < n4; i += blockDim.x) reinterpret_cast<float4*>(t)[i] = __ldg(src + i);
         __syncthreads();
         rtab = t;
-    } else if constexpr (std::is_same<R, double>::value && S::N <= 2) {
-        // FP64 Boys interval polynomials for the closed-form roots
-        double* t = fast_smem + S::SMEM_DOUBLES;
-        const int n2 = c_tabs.boys_iv_nint[S::N] * kBoysIvCoefDev / 2;
-        const double2* src = reinterpret_cast<const double2*>(c_tabs.boys_iv[S::N]);
-        for (int i = threadIdx.x; i < n2; i += blockDim.x) reinterpret_cast<double2*>(t)[i] = __ldg(src + i);
+    } else if constexpr (S::N == 1) {
+        // FP64 N = 1: the reference's raw grid rows (root, weight)
+        double2* t = reinterpret_cast<double2*>(fast_smem + S::SMEM_DOUBLES);
+        const double2* src = reinterpret_cast<const double2*>(c_tabs.rys_raw1);
+        for (int i = threadIdx.x; i < c_tabs.rys_raw1_rows; i += blockDim.x) t[i] = __ldg(src + i);
         __syncthreads();
         rtab = t;
     }
@@ -513,6 +516,28 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                 for (int d = 0; d < S::NSD; ++d) kadc[a][d] = 0.0;
             }
         }
+        // The bras of a block share shell A, so the lane's D[a, c], D[a, d]
+        // and D[c, d] are the same for every bra of it: the FP32 kernels (whose
+        // registers allow it) gather them once per tile.
+        constexpr bool PRE = CARRY && std::is_same<R, float>::value;
+        R pdac[PRE ? S::NSA : 1][PRE ? S::NSC : 1], pdad[PRE ? S::NSA : 1][PRE ? S::NSD : 1];
+        R pdcd[PRE ? S::NSCD : 1];
+        if constexpr (PRE) {
+            const int a0b = __ldg(pv.shell_sph + __ldg(pv.pair_A + __ldg(cl.bra_list + bd.bra0)));
+            if (cl.want_k) {
+#pragma unroll
+                for (int sa = 0; sa < S::NSA; ++sa) {
+#pragma unroll
+                    for (int sc = 0; sc < S::NSC; ++sc) pdac[sa][sc] = dm(a0b + sa, c0 + sc);
+#pragma unroll
+                    for (int sd = 0; sd < S::NSD; ++sd) pdad[sa][sd] = dm(a0b + sa, d0 + sd);
+                }
+            }
+            if (cl.want_j) {
+#pragma unroll
+                for (int t = 0; t < S::NSCD; ++t) pdcd[t] = dm(c0 + t / S::NSD, d0 + t % S::NSD);
+            }
+        }
         bool touched = false;
         int a0 = 0;
 
@@ -617,20 +642,36 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS)
                                 jcd[t] += fj * s;
                             else
                                 atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, double(fj * s));
-                            const R dcd = R(dm(c0 + sc, d0 + sd));
+                            R dcd;
+                            if constexpr (PRE) dcd = pdcd[t];
+                            else dcd = R(dm(c0 + sc, d0 + sd));
 #pragma unroll
                             for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
                         }
                         if (cl.want_k) {
+                            // D[b, d] and D[b, c] of this column, gathered once
+                            R dbd[S::NSB], dbc[S::NSB];
+#pragma unroll
+                            for (int sb = 0; sb < S::NSB; ++sb) {
+                                dbd[sb] = R(dm(b0 + sb, d0 + sd));
+                                dbc[sb] = R(dm(b0 + sb, c0 + sc));
+                            }
 #pragma unroll
                             for (int sa = 0; sa < S::NSA; ++sa) {
-                                const R dad = R(dm(a0 + sa, d0 + sd)), dac = R(dm(a0 + sa, c0 + sc));
+                                R dad, dac;
+                                if constexpr (PRE) {
+                                    dad = pdad[sa][sd];
+                                    dac = pdac[sa][sc];
+                                } else {
+                                    dad = R(dm(a0 + sa, d0 + sd));
+                                    dac = R(dm(a0 + sa, c0 + sc));
+                                }
                                 R sac = R(0), sad = R(0);
 #pragma unroll
                                 for (int sb = 0; sb < S::NSB; ++sb) {
                                     const R v = V[sa * S::NSB + sb];
-                                    sac += v * R(dm(b0 + sb, d0 + sd));
-                                    sad += v * R(dm(b0 + sb, c0 + sc));
+                                    sac += v * dbd[sb];
+                                    sad += v * dbc[sb];
                                     kbc[sb] += v * dad;
                                     kbd[sb][sd] += v * dac;
                                 }

@@ -175,29 +175,17 @@ __global__ void rys_test_kernel(const double* T, int n, int nroots, double* root
     }
 }
 
-// Test hook of the shared-memory root paths, reading the tables from global
-// memory: mode 2 = FP32 interval polynomials (N <= 3), mode 3 = FP64 closed
-// forms from the Boys interval polynomials (N <= 2).
+// Test hook of the FP32 shared-memory root path (mode 2), reading the
+// interval polynomials from global memory.
 template <int N>
 __global__ void rys_interval_test_kernel(const double* T, int n, int mode, double* roots, double* weights) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (mode == 2) {
-        float r[N], w[N];
-        rys_roots_smem32<N>(float(T[i]), c_tabs.rys32[N], r, w);
-        for (int k = 0; k < N; ++k) {
-            roots[(long long)i * N + k] = r[k];
-            weights[(long long)i * N + k] = w[k];
-        }
-    } else {
-        if constexpr (N <= 2) {
-            double r[N], w[N];
-            rys_roots_boys<N>(T[i], c_tabs.boys_iv[N], r, w);
-            for (int k = 0; k < N; ++k) {
-                roots[(long long)i * N + k] = r[k];
-                weights[(long long)i * N + k] = w[k];
-            }
-        }
+    if (i >= n || mode != 2) return;
+    float r[N], w[N];
+    rys_roots_smem32<N>(float(T[i]), c_tabs.rys32[N], r, w);
+    for (int k = 0; k < N; ++k) {
+        roots[(long long)i * N + k] = r[k];
+        weights[(long long)i * N + k] = w[k];
     }
 }
 
@@ -436,10 +424,16 @@ void ensure_device_tables() {
         t.rys32[n] = upload(rys32_table(n));
         t.rys32_nint[n] = rys32_intervals(n);
     }
-    for (int n = 1; n <= 2; ++n) {
-        t.boys_iv[n] = upload(boys_iv_table(n));
-        t.boys_iv_nint[n] = boys_iv_intervals(n);
+    {
+        std::vector<double> raw(2 * static_cast<std::size_t>(h.rys_rows[1]));
+        for (int k = 0; k < h.rys_rows[1]; ++k) {
+            raw[2 * k] = h.rys_roots[1][k];
+            raw[2 * k + 1] = h.rys_weights[1][k];
+        }
+        t.rys_raw1 = upload(raw);
+        t.rys_raw1_rows = h.rys_rows[1];
     }
+
     CartTable ct{};
     build_cart(ct);
     C2STable c2s{};

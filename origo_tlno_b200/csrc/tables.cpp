@@ -246,65 +246,7 @@ bool rys_rule_accurate(int n, double t, double* roots, double* weights) {
     return true;
 }
 
-namespace {
-// Chebyshev nodes u_j of [-1/2, 1/2] (nc of them) and the inverse of their
-// Vandermonde matrix (monomials in u, lowest power first), long double:
-// coefficient c = sum_j inv[c][j] f(u_j) interpolates f at the nodes.
-void chebyshev_fit_matrix(int nc, std::vector<long double>& nodes, std::vector<long double>& inv) {
-    nodes.resize(nc);
-    for (int j = 0; j < nc; ++j)
-        nodes[j] = 0.5L * std::cos((2.0L * j + 1.0L) * 3.14159265358979323846264338327950288L / (2.0L * nc));
-    std::vector<long double> A(static_cast<std::size_t>(nc) * 2 * nc, 0.0L);
-    auto a = [&](int r, int c) -> long double& { return A[static_cast<std::size_t>(r) * 2 * nc + c]; };
-    for (int r = 0; r < nc; ++r) {
-        long double pw = 1.0L;
-        for (int c = 0; c < nc; ++c) { a(r, c) = pw; pw *= nodes[r]; }
-        a(r, nc + r) = 1.0L;
-    }
-    for (int c = 0; c < nc; ++c) {  // Gauss-Jordan with partial pivoting
-        int piv = c;
-        for (int r = c + 1; r < nc; ++r)
-            if (std::fabs(a(r, c)) > std::fabs(a(piv, c))) piv = r;
-        for (int k = 0; k < 2 * nc; ++k) std::swap(a(c, k), a(piv, k));
-        const long double d = a(c, c);
-        for (int k = 0; k < 2 * nc; ++k) a(c, k) /= d;
-        for (int r = 0; r < nc; ++r) {
-            if (r == c) continue;
-            const long double f = a(r, c);
-            for (int k = 0; k < 2 * nc; ++k) a(r, k) -= f * a(c, k);
-        }
-    }
-    inv.assign(static_cast<std::size_t>(nc) * nc, 0.0L);
-    for (int c = 0; c < nc; ++c)
-        for (int j = 0; j < nc; ++j) inv[static_cast<std::size_t>(c) * nc + j] = a(c, nc + j);
-}
-}  // namespace
-
-int boys_iv_intervals(int n_roots) { return static_cast<int>(std::ceil(rys_tmax(n_roots) * kBoysIvPerUnit)); }
-
-std::vector<double> boys_iv_table(int n_roots) {
-    constexpr int nc = kBoysIvDeg + 1;
-    const int m = 2 * n_roots - 1;
-    const int nint = boys_iv_intervals(n_roots);
-    std::vector<long double> un, inv;
-    chebyshev_fit_matrix(nc, un, inv);
-    std::vector<double> out(static_cast<std::size_t>(nint) * nc, 0.0);
-    const double h = 1.0 / kBoysIvPerUnit;
-    std::vector<double> F(m + 1);
-    for (int k = 0; k < nint; ++k) {
-        double vals[nc];
-        for (int j = 0; j < nc; ++j) {
-            boys_quadrature(m, (k + 0.5 + static_cast<double>(un[j])) * h, F.data());
-            vals[j] = F[m];
-        }
-        for (int c = 0; c < nc; ++c) {
-            long double acc = 0.0L;
-            for (int j = 0; j < nc; ++j) acc += inv[static_cast<std::size_t>(c) * nc + j] * vals[j];
-            out[static_cast<std::size_t>(k) * nc + c] = static_cast<double>(acc);
-        }
-    }
-    return out;
-}
+int rys_rows(int n) { return static_cast<int>(rys_tmax(n) * 100.0) + 7; }
 
 int rys32_intervals(int n) { return static_cast<int>(std::ceil(rys_tmax(n) * kRys32PerUnit)); }
 
@@ -375,7 +317,7 @@ const HostTables& host_tables() {
         std::vector<std::string> errors(kRysMaxN + 1);
         for (int n = 1; n <= kRysMaxN; ++n) {
             tabs.rys_tmax[n] = rys_tmax(n);
-            tabs.rys_rows[n] = static_cast<int>(rys_tmax(n) * 100.0) + 7;
+            tabs.rys_rows[n] = rys_rows(n);
             tabs.rys_roots[n].assign(static_cast<std::size_t>(tabs.rys_rows[n]) * n, 0.0);
             tabs.rys_weights[n].assign(static_cast<std::size_t>(tabs.rys_rows[n]) * n, 0.0);
         }

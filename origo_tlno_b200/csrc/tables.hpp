@@ -48,16 +48,9 @@ constexpr int kRys32Deg = 5;
 int rys32_intervals(int n);
 std::vector<float> rys32_table(int n);
 
-// FP64 Boys interval polynomials of the N <= 2 root classes: F_m(T), m =
-// 2N - 1, on each interval [k h, (k+1) h) of [0, tmax(N)), h = 1 /
-// kBoysIvPerUnit, as a degree-kBoysIvDeg polynomial in u = T / h - k - 1/2,
-// interpolating the Gauss-Legendre quadrature of F_m at the Chebyshev nodes
-// of the interval (error below 3e-15 relative).  Record k:
-// [k * (kBoysIvDeg + 1) + j], lowest power first.
-constexpr int kBoysIvPerUnit = 4;
-constexpr int kBoysIvDeg = 9;
-int boys_iv_intervals(int n_roots);
-std::vector<double> boys_iv_table(int n_roots);
+// Rows of the Rys grid of root count n (tmax(n) / 0.01 + 7 guard rows for
+// the 5-point stencil).
+int rys_rows(int n);
 
 // Builds (once per process, thread-safe) and returns the tables.
 const HostTables& host_tables();

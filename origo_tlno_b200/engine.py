@@ -505,7 +505,7 @@ def boys(x, maxn: int, device: int = 0) -> np.ndarray:
     return out
 
 
-RYS_PATHS = {"fp64_table": 0, "fp32_table": 1, "fp32_interval": 2, "fp64_boys": 3}
+RYS_PATHS = {"fp64_table": 0, "fp32_table": 1, "fp32_interval": 2}
 
 
 def rys_roots(T, nroots: int, fp32: bool = False, device: int = 0, path: Optional[str] = None):

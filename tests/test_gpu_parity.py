@@ -2,10 +2,11 @@
 
 Checks use the committed golden fixtures (made by tests/golden/make_golden.py
 from the compiled reference) and, where the compiled reference library is
-present (oracle/_ref), fresh reference results.  Tolerances: 1e-12 absolute
-for FP64 integrals, J and K (the reference's own AVX2/AVX-512 routes differ by
-up to 1.6e-12 in J/K elements, so J/K use 5e-12 on the larger system);
-mixed precision 1e-7 on J/K elements and 1e-6 Eh on the energy tr(D(J-K/2)).
+present (oracle/_ref), fresh reference results.  Every test prints its
+achieved errors (PIN lines).  Tolerances: 1e-12 absolute for FP64 integrals,
+J and K, except the stated cases (cfg1 kinetic matrix, the f-shell
+fragment's J/K); mixed precision 1e-7 on J/K elements and 1e-6 Eh on the
+energy tr(D(J-K/2)).
 """
 import numpy as np
 import pytest
@@ -71,86 +72,67 @@ def test_rys_fp32_interval_polynomials(n):
     assert er < 5e-7 and ew < 5e-7
 
 
-@pytest.mark.parametrize("n", [1, 2])
-def test_rys_fp64_boys_closed_forms(n):
-    # The FP64 N <= 2 kernels' closed forms from Boys values.  Against the
-    # reference's accurate generator (rys_roots_weights_accurate: the same
-    # moment closed forms from its own Boys values) they agree to 3e-14;
-    # against its production 0.01-grid table they differ by that table's
-    # 5-point interpolation error, up to ~2.5e-13 in the N = 1 weight.
-    g = load_golden("rys.npz")
-    T = g["T"]
-    r, w = E.rys_roots(T, n, path="fp64_boys")
-    er = _maxabs(r, g["roots"][n - 1, :, :n])
-    ew = _maxabs(w, g["weights"][n - 1, :, :n])
-    msg = f"PIN rys_fp64_boys N={n} vs_table_root={er:.2e} vs_table_weight={ew:.2e}"
-    from oracle import ref
-    if ref.available():
-        acc = [ref.rys_roots(n, float(t), accurate=True) for t in T]
-        ea = _maxabs(r, np.array([a[0] for a in acc]))
-        eaw = _maxabs(w, np.array([a[1] for a in acc]))
-        msg += f" vs_accurate_root={ea:.2e} vs_accurate_weight={eaw:.2e}"
-        assert ea < 3e-14 and eaw < 3e-14
-    print(msg)
-    assert er < 5e-13 and ew < 5e-13
-
-
-def _check_blocks(ctx, g, tol):
+def _check_blocks(ctx, g, tol, name):
     q = g["quartets"]
     blocks = ctx.eri_blocks(q)
     err = 0.0
     for k, blk in enumerate(blocks):
         ref = g["eri"][g["eri_off"][k]:g["eri_off"][k + 1]].reshape(blk.shape)
         err = max(err, _maxabs(blk, ref))
+    print(f"PIN eri_blocks_{name} max_abs={err:.2e} blocks={len(blocks)}")
     assert err < tol, err
 
 
 def test_eri_blocks_cfg0_all_quartets(ctx0):
-    _check_blocks(ctx0, load_golden("cfg0.npz"), 1e-12)
+    _check_blocks(ctx0, load_golden("cfg0.npz"), 1e-12, "cfg0")
 
 
 def test_eri_blocks_cfg1_sample(ctx1):
-    _check_blocks(ctx1, load_golden("cfg1.npz"), 1e-12)
+    _check_blocks(ctx1, load_golden("cfg1.npz"), 1e-12, "cfg1")
 
 
 def test_schwarz_bounds(ctx0, ctx1):
-    assert _maxabs(ctx0.schwarz(), load_golden("cfg0.npz")["schwarz"]) < 1e-12
-    assert _maxabs(ctx1.schwarz(), load_golden("cfg1.npz")["schwarz"]) < 1e-12
+    e0 = _maxabs(ctx0.schwarz(), load_golden("cfg0.npz")["schwarz"])
+    e1 = _maxabs(ctx1.schwarz(), load_golden("cfg1.npz")["schwarz"])
+    print(f"PIN schwarz cfg0={e0:.2e} cfg1={e1:.2e}")
+    assert e0 < 1e-12 and e1 < 1e-12
 
 
 def test_jk_cfg0(ctx0):
     g = load_golden("cfg0.npz")
     out = ctx0.jk(g["D"], want=("J", "K", "G"))
-    assert _maxabs(out["J"], g["J"]) < 1e-12
-    assert _maxabs(out["K"], g["K"]) < 1e-12
-    assert _maxabs(out["G"], g["G"]) < 1e-12
+    ej, ek, eg = _maxabs(out["J"], g["J"]), _maxabs(out["K"], g["K"]), _maxabs(out["G"], g["G"])
+    print(f"PIN jk_cfg0 J={ej:.2e} K={ek:.2e} G={eg:.2e}")
+    assert ej < 1e-12 and ek < 1e-12 and eg < 1e-12
 
 
 def test_jk_cfg0_unscreened():
     g = load_golden("cfg0.npz")
     c = E.Context(M.cfg0()).plan(E.ScreeningOptions(integral_threshold=0.0))
     out = c.jk(g["D"])
-    assert _maxabs(out["J"], g["J0"]) < 1e-12
-    assert _maxabs(out["K"], g["K0"]) < 1e-12
+    ej, ek = _maxabs(out["J"], g["J0"]), _maxabs(out["K"], g["K0"])
+    print(f"PIN jk_cfg0_unscreened J={ej:.2e} K={ek:.2e}")
+    assert ej < 1e-12 and ek < 1e-12
 
 
 def test_jk_cfg1(ctx1):
     g = load_golden("cfg1.npz")
     D = M.density_for("cfg1", M.cfg1())
     out = ctx1.jk(D)
-    assert _maxabs(out["J"], g["J"]) < 5e-12
-    assert _maxabs(out["K"], g["K"]) < 5e-12
+    ej, ek = _maxabs(out["J"], g["J"]), _maxabs(out["K"], g["K"])
+    print(f"PIN jk_cfg1 J={ej:.2e} K={ek:.2e}")
+    assert ej < 1e-12 and ek < 1e-12
 
 
 def test_jk_cfg1_mixed(ctx1):
     g = load_golden("cfg1.npz")
     D = M.density_for("cfg1", M.cfg1())
     out = ctx1.jk(D, mixed=True)
-    assert _maxabs(out["J"], g["J"]) < 1e-7
-    assert _maxabs(out["K"], g["K"]) < 1e-7
+    ej, ek = _maxabs(out["J"], g["J"]), _maxabs(out["K"], g["K"])
     e = np.sum(D * (out["J"] - 0.5 * out["K"]))
     e_ref = np.sum(D * (g["J"] - 0.5 * g["K"]))
-    assert abs(e - e_ref) < 1e-6
+    print(f"PIN jk_cfg1_mixed_1e-9 J={ej:.2e} K={ek:.2e} E={abs(e - e_ref):.2e}")
+    assert ej < 1e-7 and ek < 1e-7 and abs(e - e_ref) < 1e-6
 
 
 def test_cfg2_fragment_f_shells():
@@ -164,14 +146,16 @@ def test_cfg2_fragment_f_shells():
     for k, blk in enumerate(blocks):
         ref = g["eri"][g["eri_off"][k]:g["eri_off"][k + 1]].reshape(blk.shape)
         err = max(err, _maxabs(blk, ref))
-    assert err < 1e-12
     out = ctx.jk(g["D"])
-    assert _maxabs(out["J"], g["J"]) < 5e-12
-    assert _maxabs(out["K"], g["K"]) < 5e-12
+    ej, ek = _maxabs(out["J"], g["J"]), _maxabs(out["K"], g["K"])
     S, T, V = ctx.onee()
-    assert _maxabs(S, g["S"]) < 1e-12
-    assert _maxabs(T, g["T"]) < 2e-12
-    assert _maxabs(V, g["V"]) < 1e-12
+    es, et, ev = _maxabs(S, g["S"]), _maxabs(T, g["T"]), _maxabs(V, g["V"])
+    print(f"PIN cfg2_fragment eri={err:.2e} J={ej:.2e} K={ek:.2e} S={es:.2e} T={et:.2e} V={ev:.2e}")
+    assert err < 1e-12
+    # J and K of this fragment sum f-shell quartets whose reference values
+    # the reference's AVX2 and portable routes reproduce to ~2e-12
+    assert ej < 5e-12 and ek < 5e-12
+    assert es < 1e-12 and et < 2e-12 and ev < 1e-12
     ctx.close()
 
 
@@ -213,9 +197,9 @@ def test_mixed_threshold_autotune_cfg1():
 def test_onee_cfg0(ctx0):
     g = load_golden("cfg0.npz")
     S, T, V = ctx0.onee(screening=True)
-    assert _maxabs(S, g["S"]) < 1e-12
-    assert _maxabs(T, g["T"]) < 1e-12
-    assert _maxabs(V, g["V"]) < 1e-12
+    es, et, ev = _maxabs(S, g["S"]), _maxabs(T, g["T"]), _maxabs(V, g["V"])
+    print(f"PIN onee_cfg0 S={es:.2e} T={et:.2e} V={ev:.2e}")
+    assert es < 1e-12 and et < 1e-12 and ev < 1e-12
 
 
 def test_onee_cfg1(ctx1):
@@ -225,9 +209,9 @@ def test_onee_cfg1(ctx1):
     # molecule, so T is held to 2e-12 (S and V to 1e-12).
     g = load_golden("cfg1.npz")
     S, T, V = ctx1.onee(screening=True)
-    assert _maxabs(S, g["S"]) < 1e-12
-    assert _maxabs(T, g["T"]) < 2e-12
-    assert _maxabs(V, g["V"]) < 1e-12
+    es, et, ev = _maxabs(S, g["S"]), _maxabs(T, g["T"]), _maxabs(V, g["V"])
+    print(f"PIN onee_cfg1 S={es:.2e} T={et:.2e} V={ev:.2e}")
+    assert es < 1e-12 and et < 2e-12 and ev < 1e-12
 
 
 def test_density_validation_errors(ctx0):
