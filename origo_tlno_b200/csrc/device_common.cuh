@@ -31,11 +31,6 @@ struct DevTables {
     // (lowest power of u = 4T - k - 1/2 first); staged in shared memory.
     const float* rys32[4];
     int rys32_nint[4];
-    // The reference's raw 0.01-grid values for N = 1, one (root, weight)
-    // pair per grid row (46.5 KB), staged in shared memory by the FP64 N = 1
-    // kernels.
-    const double* rys_raw1;
-    int rys_raw1_rows;
 };
 constexpr int kRys32PerUnitDev = 4;
 constexpr int kRys32CoefDev = 6;
@@ -199,34 +194,6 @@ __device__ __forceinline__ void rys_roots_all(R T, R* root, R* weight) {
         v = v * t + c[0][i];
         if (i < N) root[i] = v; else weight[i - N] = v;
     }
-}
-
-// FP64 root and weight for N = 1 from the raw grid rows in shared memory
-// (f_k = (t^2, w) at T = 0.01 k), with the reference's 5-point
-// Newton-forward stencil over rows k..k+4 written out as it evaluates it
-// (rys_engine.ipp:3784-3812); the Hermite asymptotic form above tmax(1).
-__device__ __forceinline__ void rys_root1_raw(double T, const double2* __restrict__ rows, double& root,
-                                              double& weight) {
-    if (T >= c_tabs.tmax[1]) {
-        const double inv = 1.0 / T;
-        root = c_tabs.h2[1][0] * inv;
-        weight = c_tabs.hw[1][0] * sqrt(inv);
-        return;
-    }
-    const double fi = T * 100.0;
-    const int k = static_cast<int>(fi);
-    const double t = fi - k;
-    const double tm1 = t - 1.0, tm2 = t - 2.0, tm3 = t - 3.0;
-    const double2 f0 = rows[k], f1 = rows[k + 1], f2 = rows[k + 2], f3 = rows[k + 3], f4 = rows[k + 4];
-    auto newton = [&](double a0, double a1, double a2, double a3, double a4) {
-        const double d1 = a1 - a0;
-        const double d2 = (a2 - 2.0 * a1 + a0) * 0.5;
-        const double d3 = (a3 - 3.0 * a2 + 3.0 * a1 - a0) * (1.0 / 6.0);
-        const double d4 = (a4 - 4.0 * a3 + 6.0 * a2 - 4.0 * a1 + a0) * (1.0 / 24.0);
-        return a0 + t * (d1 + tm1 * (d2 + tm2 * (d3 + tm3 * d4)));
-    };
-    root = newton(f0.x, f1.x, f2.x, f3.x, f4.x);
-    weight = newton(f0.y, f1.y, f2.y, f3.y, f4.y);
 }
 
 // FP32 roots and weights for N <= 3 from the shared-memory interval

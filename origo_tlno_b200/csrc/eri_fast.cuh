@@ -113,6 +113,9 @@ struct FastShape {
     static constexpr int GB = (TPQ == 1 && NSA * (NSC + NSD) + NSCD <= kMaxCarried) ? kBraGroup : 1;
     static constexpr int LANE_STRIDE = (NAS * NSCD) | 1;  // odd: conflict-free FP64 rows
     static constexpr int SMEM_DOUBLES = TPQ == 1 ? 0 : BBQ * 32 * LANE_STRIDE;
+    // Bra-group classes: per lane, the density values every bra of a block
+    // shares (D[a,c], D[a,d], D[c,d]), gathered once per tile.
+    static constexpr int PRE_VALS = GB > 1 ? NSA * NSC + NSA * NSD + NSCD : 0;
 };
 
 // Binomial C(n, k) for the small HRR exponents.
@@ -196,11 +199,7 @@ struct QuartetGeom {
 // Phase 1 + 2 for slice G (rows ia = G, G+TPQ, ...).
 template <typename R, int LA, int LB, int LC, int LD, int G>
 __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket, bool active, const QuartetGeom& q,
-                                           double fs_thr2, const void* rtab_v, R* __restrict__ ks) {
-    // shared-memory root tables: FP32 interval polynomials (FP32, N <= 3) or
-    // the raw N = 1 grid (FP64, N = 1)
-    const float* rtab = static_cast<const float*>(rtab_v);
-    const double2* rtab64 = static_cast<const double2*>(rtab_v);
+                                           double fs_thr2, const float* rtab, R* __restrict__ ks) {
     using S = FastShape<LA, LB, LC, LD>;
     constexpr int ROWS = (S::NAS - G + S::TPQ - 1) / S::TPQ;
     R acc[ROWS > 0 ? ROWS : 1][S::NCS];
@@ -276,8 +275,6 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
                         rt[r] = R(rd[r]);
                         wt[r] = R(wd[r]);
                     }
-                } else if constexpr (S::N == 1) {
-                    rys_root1_raw(Targ, rtab64, rt[0], wt[0]);
                 } else {
                     rys_roots_all<R, S::N>(Targ, rt, wt);
                 }
@@ -347,7 +344,7 @@ __device__ __forceinline__ void fast_slice(const PlanView& pv, int bra, int ket,
 
 template <typename R, int LA, int LB, int LC, int LD, int G = 0>
 __device__ __forceinline__ void fast_slice_dispatch(int g, const PlanView& pv, int bra, int ket, bool active,
-                                                    const QuartetGeom& q, double fs_thr2, const void* rtab,
+                                                    const QuartetGeom& q, double fs_thr2, const float* rtab,
                                                     R* ks) {
     using S = FastShape<LA, LB, LC, LD>;
     if constexpr (G < S::TPQ) {
@@ -373,13 +370,31 @@ __device__ __forceinline__ bool group_any(bool pred, int id, int nthreads) {
     return r != 0;
 }
 
-// Unsliced classes are latency-bound on their gathers: the register cap of
-// 4 resident CTAs per SM (FP64) or 6 (FP32) buys more warps than it costs in
-// spills (measured on the six s/p classes of 200 waters: 589 -> 561 ms FP64,
-// 372 -> 364 ms FP32 summed).
+// The lightest classes (at most 9 radial accumulators per thread) are
+// latency-bound on their gathers: a register cap of 4 resident CTAs per SM
+// (FP64) or 6 (FP32) buys more warps than it costs (measured on 200 waters);
+// classes with larger accumulator blocks would spill under it.
 template <typename R, int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
-                                  FastShape<LA, LB, LC, LD>::TPQ == 1 ? (std::is_same<R, float>::value ? 6 : 4) : 1)
+__host__ __device__ constexpr int fast_min_blocks() {
+    using S = FastShape<LA, LB, LC, LD>;
+    return (S::TPQ == 1 && S::NAS * S::NCS <= 9) ? (std::is_same<R, float>::value ? 6 : 4) : 1;
+}
+
+// Where a bra-group class keeps the per-tile density values of a lane:
+// 0 none (no bra groups), 1 registers, 2 shared memory.  Shared memory where
+// registers are tight (FP64, and the capped FP32 classes: 3-10% faster on the
+// s/p classes of 400 waters); registers for the uncapped FP32 classes, where
+// the extra shared memory costs resident CTAs (+18% on (pp|ps)).
+template <typename R, int LA, int LB, int LC, int LD>
+__host__ __device__ constexpr int fast_pre_mode() {
+    using S = FastShape<LA, LB, LC, LD>;
+    if (S::PRE_VALS == 0) return 0;
+    if (std::is_same<R, double>::value) return 2;
+    return fast_min_blocks<R, LA, LB, LC, LD>() > 1 ? 2 : 1;
+}
+
+template <typename R, int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS, fast_min_blocks<R, LA, LB, LC, LD>())
     eri_fast_jk_kernel(PlanView pv, ClassLaunch cl) {
     using S = FastShape<LA, LB, LC, LD>;
     extern __shared__ double fast_smem[];
@@ -397,7 +412,8 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
     const int bar_id = 1 + grp, bar_n = 32 * S::TPQ;
     // FP32 kernels with N <= 3 stage their Rys interval polynomials in shared
     // memory behind the row-exchange buffer.
-    const void* rtab = nullptr;
+    const float* rtab = nullptr;
+    int smem_used = S::SMEM_DOUBLES * 8;  // bytes
     if constexpr (std::is_same<R, float>::value && S::N <= 3) {
         float* t = reinterpret_cast<float*>(fast_smem + S::SMEM_DOUBLES);
         const int n4 = c_tabs.rys32_nint[S::N] * (kRys32CoefDev * 2 * S::N) / 4;
@@ -405,14 +421,12 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
         for (int i = threadIdx.x; i < n4; i += blockDim.x) reinterpret_cast<float4*>(t)[i] = __ldg(src + i);
         __syncthreads();
         rtab = t;
-    } else if constexpr (S::N == 1) {
-        // FP64 N = 1: the reference's raw grid rows (root, weight)
-        double2* t = reinterpret_cast<double2*>(fast_smem + S::SMEM_DOUBLES);
-        const double2* src = reinterpret_cast<const double2*>(c_tabs.rys_raw1);
-        for (int i = threadIdx.x; i < c_tabs.rys_raw1_rows; i += blockDim.x) t[i] = __ldg(src + i);
-        __syncthreads();
-        rtab = t;
+        smem_used += n4 * 16;
     }
+    // this warp's slots of the per-tile density values (shared-memory mode)
+    constexpr int PRE_MODE = fast_pre_mode<R, LA, LB, LC, LD>();
+    R* pre = reinterpret_cast<R*>(reinterpret_cast<unsigned char*>(fast_smem) + smem_used) +
+             (PRE_MODE == 2 ? warp * 32 * S::PRE_VALS : 0);
     __shared__ int s_chunk[S::BBQ];
     const int ntiles = cl.tile_end - cl.tile_begin;
     double csum = 0.0;  // ERI checksum stream: this thread's share
@@ -517,25 +531,31 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
             }
         }
         // The bras of a block share shell A, so the lane's D[a, c], D[a, d]
-        // and D[c, d] are the same for every bra of it: the FP32 kernels (whose
-        // registers allow it) gather them once per tile.
-        constexpr bool PRE = CARRY && std::is_same<R, float>::value;
-        R pdac[PRE ? S::NSA : 1][PRE ? S::NSC : 1], pdad[PRE ? S::NSA : 1][PRE ? S::NSD : 1];
-        R pdcd[PRE ? S::NSCD : 1];
+        // and D[c, d] are the same for every bra of it: they are gathered once
+        // per tile, into registers or this lane's shared-memory slots
+        // [k * 32 + lane].
+        constexpr bool PRE = PRE_MODE != 0;
+        R preg[PRE_MODE == 1 ? S::PRE_VALS : 1];
+        auto pre_at = [&](int k) -> R& {
+            if constexpr (PRE_MODE == 1) return preg[k];
+            else return pre[k * 32 + lane];
+        };
         if constexpr (PRE) {
             const int a0b = __ldg(pv.shell_sph + __ldg(pv.pair_A + __ldg(cl.bra_list + bd.bra0)));
             if (cl.want_k) {
 #pragma unroll
                 for (int sa = 0; sa < S::NSA; ++sa) {
 #pragma unroll
-                    for (int sc = 0; sc < S::NSC; ++sc) pdac[sa][sc] = dm(a0b + sa, c0 + sc);
+                    for (int sc = 0; sc < S::NSC; ++sc) pre_at(sa * S::NSC + sc) = dm(a0b + sa, c0 + sc);
 #pragma unroll
-                    for (int sd = 0; sd < S::NSD; ++sd) pdad[sa][sd] = dm(a0b + sa, d0 + sd);
+                    for (int sd = 0; sd < S::NSD; ++sd)
+                        pre_at(S::NSA * S::NSC + sa * S::NSD + sd) = dm(a0b + sa, d0 + sd);
                 }
             }
             if (cl.want_j) {
 #pragma unroll
-                for (int t = 0; t < S::NSCD; ++t) pdcd[t] = dm(c0 + t / S::NSD, d0 + t % S::NSD);
+                for (int t = 0; t < S::NSCD; ++t)
+                    pre_at(S::NSA * (S::NSC + S::NSD) + t) = dm(c0 + t / S::NSD, d0 + t % S::NSD);
             }
         }
         bool touched = false;
@@ -643,7 +663,7 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
                             else
                                 atomicAdd(Jm + (long long)(c0 + sc) * M + d0 + sd, double(fj * s));
                             R dcd;
-                            if constexpr (PRE) dcd = pdcd[t];
+                            if constexpr (PRE) dcd = pre_at(S::NSA * (S::NSC + S::NSD) + t);
                             else dcd = R(dm(c0 + sc, d0 + sd));
 #pragma unroll
                             for (int e = 0; e < S::NSAB; ++e) jab[e] += V[e] * dcd;
@@ -660,8 +680,8 @@ __global__ void __launch_bounds__(32 * FastShape<LA, LB, LC, LD>::WARPS,
                             for (int sa = 0; sa < S::NSA; ++sa) {
                                 R dad, dac;
                                 if constexpr (PRE) {
-                                    dad = pdad[sa][sd];
-                                    dac = pdac[sa][sc];
+                                    dad = pre_at(S::NSA * S::NSC + sa * S::NSD + sd);
+                                    dac = pre_at(sa * S::NSC + sc);
                                 } else {
                                     dad = R(dm(a0 + sa, d0 + sd));
                                     dac = R(dm(a0 + sa, c0 + sc));
@@ -765,6 +785,12 @@ template <int LA, int LB, int LC, int LD>
 constexpr int fast_smem_bytes() { return FastShape<LA, LB, LC, LD>::SMEM_DOUBLES * 8; }
 template <int LA, int LB, int LC, int LD>
 constexpr int fast_roots() { return FastShape<LA, LB, LC, LD>::N; }
+template <int LA, int LB, int LC, int LD>
+constexpr int fast_pre_bytes(bool fp32) {
+    using S = FastShape<LA, LB, LC, LD>;
+    return fp32 ? (fast_pre_mode<float, LA, LB, LC, LD>() == 2 ? S::WARPS * 32 * S::PRE_VALS * 4 : 0)
+                : (fast_pre_mode<double, LA, LB, LC, LD>() == 2 ? S::WARPS * 32 * S::PRE_VALS * 8 : 0);
+}
 
 }  // namespace dev
 }  // namespace tlno_gpu

@@ -15,15 +15,15 @@
 
 namespace tlno_gpu {
 
-// Dynamic shared memory: the row-exchange buffer of a sliced class, plus the
-// FP32 Rys interval polynomials in the FP32 kernels with N <= 3 and the raw
-// N = 1 grid in the FP64 N = 1 kernels.
+// Dynamic shared memory: the row-exchange buffer of a sliced class, the FP32
+// Rys interval polynomials in the FP32 kernels with N <= 3, and the per-tile
+// density slots of the bra-group classes.
 #define TLNO_FAST_IMPL(id, a, b, c, d)                                                                  \
     static int fast_smem_##id(bool fp32) {                                                              \
         constexpr int n = dev::fast_roots<a, b, c, d>();                                                \
         int bytes = dev::fast_smem_bytes<a, b, c, d>();                                                 \
         if (fp32 && n <= kRys32MaxN) bytes += rys32_intervals(n) * (kRys32Deg + 1) * 2 * n * 4;         \
-        if (!fp32 && n == 1) bytes += rys_rows(1) * 16;                                                 \
+        bytes += dev::fast_pre_bytes<a, b, c, d>(fp32);                                                 \
         return bytes;                                                                                   \
     }                                                                                                   \
     void fast_upload_##id(const dev::DevTables& t, const dev::CartTable& ct, const dev::C2STable& cs) {  \

@@ -424,15 +424,7 @@ void ensure_device_tables() {
         t.rys32[n] = upload(rys32_table(n));
         t.rys32_nint[n] = rys32_intervals(n);
     }
-    {
-        std::vector<double> raw(2 * static_cast<std::size_t>(h.rys_rows[1]));
-        for (int k = 0; k < h.rys_rows[1]; ++k) {
-            raw[2 * k] = h.rys_roots[1][k];
-            raw[2 * k + 1] = h.rys_weights[1][k];
-        }
-        t.rys_raw1 = upload(raw);
-        t.rys_raw1_rows = h.rys_rows[1];
-    }
+
 
     CartTable ct{};
     build_cart(ct);

@@ -307,3 +307,30 @@ def test_eri_checksum_against_reference(name, tau):
     _record(f"eri_checksum_{name}_{tau:g}", checksum=cs, reference=cs_ref, rel=rel, ms=ms)
     assert rel < 1e-13
     ctx.close()
+
+
+def test_cfg2_full_molecule_against_reference_fixture():
+    # the full cfg2 molecule (60 atoms, shells up to f, M = 1480): FP64 and
+    # mixed J/K against the reference's build stored by
+    # tests/golden/make_cfg2_golden.py (energy terms, row sums, samples)
+    path = os.path.join(os.path.dirname(__file__), "golden", "cfg2.npz")
+    if not os.path.exists(path):
+        pytest.skip("cfg2 reference fixture not generated")
+    g = np.load(path)
+    mol = M.cfg2()
+    D = M.density_for("cfg2", mol)
+    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=1e-12, mixed_threshold=1e-5))
+    i, j = g["idx"][:, 0], g["idx"][:, 1]
+    res = {}
+    for mixed in (False, True):
+        out = ctx.jk(D, mixed=mixed)
+        J, K = out["J"], out["K"]
+        res[mixed] = dict(sJ=_maxabs(J[i, j], g["J_samples"]), sK=_maxabs(K[i, j], g["K_samples"]),
+                          rJ=_maxabs(J.sum(axis=1), g["J_rows"]), rK=_maxabs(K.sum(axis=1), g["K_rows"]),
+                          dE=abs((np.sum(D * J) - 0.5 * np.sum(D * K)) - (g["trDJ"] - 0.5 * g["trDK"])))
+    _record("cfg2_full_fp64", **{k: float(v) for k, v in res[False].items()})
+    _record("cfg2_full_mixed_1e-5", **{k: float(v) for k, v in res[True].items()})
+    assert max(res[False]["sJ"], res[False]["sK"]) < 5e-12
+    assert res[False]["dE"] < 1e-9
+    assert max(res[True]["sJ"], res[True]["sK"]) < 1e-7 and res[True]["dE"] < 1e-6
+    ctx.close()
