@@ -19,7 +19,9 @@ Printed JSON (one line, rank 0):
   e2e            the same build through the host-buffer C-ABI call
                  (H2D of D, D2H of J and K inside the timed region);
   cpu_baseline   the reference engine (oracle/_ref, compiled from its
-                 sources) or the restatement, timed on a bounded sample.
+                 sources) timed on a bounded sample on one core, on both
+                 of its x86 build routes (AVX2 and AVX-512); the faster is
+                 the value, both are recorded.
 `--impl reference` times the reference's CPU J+K on a bounded sample of the
 workload instead and prints the same metric.  Multi-GPU: every rank runs
 an independent replica (the J/K build of one molecule is not sharded), so
@@ -156,6 +158,56 @@ def _reference_sample(name, seconds_target=15.0):
     return secs, desc, sample_mol, tau
 
 
+ROUTES = {"avx2": "AVX2 (-march=x86-64-v3), the reference's legacy tuned route",
+          "avx512": "AVX-512 (-march=x86-64-v4), the reference's native W8 route"}
+
+
+def _route_sample(name, route):
+    """One bounded reference sample on a reference build route: in this
+    process when it runs that route, else in a child process (one route per
+    process).  Returns (seconds, description, molecule, Schwarz threshold)."""
+    from oracle import ref
+    if route == ref.ROUTE:
+        return _reference_sample(name)
+    env = dict(os.environ, TLNO_REF_ROUTE=route)
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-sample", "--config", name],
+                       env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"{route} sample failed: {r.stderr.strip()[-300:]}")
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    secs, desc, mol, tau = out["secs"], out["desc"], None, None
+    return secs, desc, mol, tau
+
+
+def _routes_baseline(name):
+    """The reference J+K sample on both of its x86 build routes; the faster
+    route is the baseline, both are recorded."""
+    from oracle import ref
+    res = {}
+    mol = tau = desc = None
+    for route in ("avx2", "avx512"):
+        lib_ok = os.path.exists(os.path.join(ROOT, "oracle", "_ref",
+                                             "libtlno_ref.so" if route == "avx2" else "libtlno_ref_avx512.so"))
+        if not lib_ok:
+            res[route] = {"unavailable": "not built"}
+            continue
+        try:
+            secs, d, m, t = _route_sample(name, route)
+            res[route] = {"seconds": secs}
+            desc = desc or d
+            if m is not None:
+                mol, tau = m, t
+        except Exception as e:
+            res[route] = {"unavailable": str(e)[:200]}
+    if mol is None:
+        _, _, mol, tau = _reference_sample(name) if ref.available() else (None, None, None, None)
+    timed = {r: v["seconds"] for r, v in res.items() if "seconds" in v}
+    if not timed:
+        raise RuntimeError(f"no reference route could be timed: {res}")
+    best = min(timed, key=timed.get)
+    return timed[best], best, res, desc, mol, tau
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -170,8 +222,9 @@ def run_reference(args):
     times = []
     desc = None
     q = None
+    routes = None
     for i in range(args.warmup + args.steps):
-        secs, desc, mol, tau = _reference_sample(args.config)
+        secs, best, routes, desc, mol, tau = _routes_baseline(args.config)
         if q is None:
             q = _count_quartets(mol, tau)
         if i >= args.warmup:
@@ -182,7 +235,8 @@ def run_reference(args):
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": args.config, "sample": desc},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc,
+                            "route": ROUTES[best], "routes_last_step_s": routes, "host": _host_cpu()},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -446,6 +500,8 @@ def run_native(args):
         ctx.graph_capture(d_in.data_ptr(), J.data_ptr(), K.data_ptr(), mixed=mixed)
         torch.cuda.synchronize()
         ev = []
+        # NVTX range: lets a profiler select the launches of this sequence
+        torch.cuda.nvtx.range_push("jk_mixed" if mixed else "jk_fp64")
         with torch.cuda.stream(stream):
             for k in range(nd):
                 d_in.copy_(Ds[k])
@@ -458,6 +514,7 @@ def run_native(args):
                 e1.record(stream)
                 ev.append((e0, e1))
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         ms = [a.elapsed_time(b) for a, b in ev[args.warmup:]]
         return ms
 
@@ -530,12 +587,13 @@ def run_native(args):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
-            secs, desc, smol, stau = _reference_sample(args.config)
+            secs, best, routes, desc, smol, stau = _routes_baseline(args.config)
             q = _count_quartets(smol, stau)
             cpu = {"value": q / secs, "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": desc + f" ({q} quartets, {secs:.2f} s)", "host": _host_cpu(),
-                   "route": "AVX2 (-march=x86-64-v3), the reference's legacy tuned route; its G/K endpoints "
-                            "refuse more than one OpenMP thread"}
+                   "route": ROUTES[best] + " (the faster of its two x86 routes); its G/K endpoints refuse more "
+                            "than one OpenMP thread",
+                   "routes_s": routes}
         except Exception as e:  # the reference oracle may be absent
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
 
@@ -607,7 +665,12 @@ def main():
                     help="skip the incremental, ERI-stream and one-electron legs")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep --mixed-threshold instead of autotuning the split threshold")
+    ap.add_argument("--ref-sample", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.ref_sample:  # one reference sample on this process's route
+        secs, desc, _, _ = _reference_sample(args.config)
+        print(json.dumps({"secs": secs, "desc": desc}))
+        return 0
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

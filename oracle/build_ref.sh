@@ -22,8 +22,11 @@ if [ ! -d "$REF/integrals" ]; then
     echo "build_ref: reference sources not found at $REF" >&2
     exit 2
 fi
-mkdir -p "$OBJ"
+mkdir -p "$OBJ" "$OBJ/avx512"
 FLAGS=(-std=c++17 -O3 -DNDEBUG -march=x86-64-v3 -mtune=generic -fopenmp -fPIC -I"$REF" -w)
+# the reference's AVX-512 route (TLNO_SIMD=avx512: -march=x86-64-v4), built
+# into oracle/_ref/libtlno_ref_avx512.so when the host compiler accepts it
+FLAGS512=(-std=c++17 -O3 -DNDEBUG -march=x86-64-v4 -mtune=generic -fopenmp -fPIC -I"$REF" -w)
 SRCS=(
   core/shell/shell_math.cpp
   core/shell/shell_contract.cpp
@@ -44,25 +47,37 @@ SRCS=(
 )
 pids=()
 objs=()
+objs512=()
 for s in "${SRCS[@]}"; do
-  o="$OBJ/$(echo "$s" | tr '/' '_' ).o"
-  objs+=("$o")
-  if [ ! -f "$o" ] || [ "$REF/$s" -nt "$o" ]; then
-    "$CXX" "${FLAGS[@]}" -c "$REF/$s" -o "$o" &
+  b="$(echo "$s" | tr '/' '_' ).o"
+  objs+=("$OBJ/$b")
+  objs512+=("$OBJ/avx512/$b")
+  if [ ! -f "$OBJ/$b" ] || [ "$REF/$s" -nt "$OBJ/$b" ]; then
+    "$CXX" "${FLAGS[@]}" -c "$REF/$s" -o "$OBJ/$b" &
+    pids+=($!)
+  fi
+  if [ ! -f "$OBJ/avx512/$b" ] || [ "$REF/$s" -nt "$OBJ/avx512/$b" ]; then
+    "$CXX" "${FLAGS512[@]}" -c "$REF/$s" -o "$OBJ/avx512/$b" &
     pids+=($!)
   fi
 done
 for h in ref_harness ref_frontend; do
-  H="$OBJ/$h.o"
-  objs+=("$H")
-  if [ ! -f "$H" ] || [ "$HERE/$h.cpp" -nt "$H" ]; then
-    "$CXX" "${FLAGS[@]}" -c "$HERE/$h.cpp" -o "$H" &
+  objs+=("$OBJ/$h.o")
+  objs512+=("$OBJ/avx512/$h.o")
+  if [ ! -f "$OBJ/$h.o" ] || [ "$HERE/$h.cpp" -nt "$OBJ/$h.o" ]; then
+    "$CXX" "${FLAGS[@]}" -c "$HERE/$h.cpp" -o "$OBJ/$h.o" &
+    pids+=($!)
+  fi
+  if [ ! -f "$OBJ/avx512/$h.o" ] || [ "$HERE/$h.cpp" -nt "$OBJ/avx512/$h.o" ]; then
+    "$CXX" "${FLAGS512[@]}" -c "$HERE/$h.cpp" -o "$OBJ/avx512/$h.o" &
     pids+=($!)
   fi
 done
 for p in "${pids[@]}"; do wait "$p"; done
 "$CXX" -shared -fopenmp -o "$OUT/libtlno_ref.so" "${objs[@]}"
 echo "build_ref: wrote $OUT/libtlno_ref.so"
+"$CXX" -shared -fopenmp -o "$OUT/libtlno_ref_avx512.so" "${objs512[@]}"
+echo "build_ref: wrote $OUT/libtlno_ref_avx512.so"
 # The C++ shim test (tests/shim/shim_test.cpp) compiled against the
 # reference's headers, linking the compiled reference and the engine library
 # (built before this script runs).

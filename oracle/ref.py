@@ -14,7 +14,13 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_ref", "libtlno_ref.so")
+# TLNO_REF_ROUTE selects the reference build: "avx2" (its legacy tuned
+# route, -march=x86-64-v3, the default) or "avx512" (its native W8 route,
+# -march=x86-64-v4).  One route per process.
+ROUTE = os.environ.get("TLNO_REF_ROUTE", "avx2")
+if ROUTE not in ("avx2", "avx512"):
+    raise ValueError(f"TLNO_REF_ROUTE must be avx2 or avx512, not {ROUTE!r}")
+LIB_PATH = os.path.join(HERE, "_ref", "libtlno_ref.so" if ROUTE == "avx2" else "libtlno_ref_avx512.so")
 
 _lib = None
 _gomp = None

@@ -9,6 +9,7 @@ digestion.  With --once it only launches the selected classes one time each
 
     python -m origo_tlno_b200.classprof cfg4 --classes "10|00" --once
     python -m origo_tlno_b200.classprof water60 --reps 3 --fp32
+    python -m origo_tlno_b200.classprof water200 --onee
 """
 from __future__ import annotations
 
@@ -41,6 +42,9 @@ def main(argv=None) -> int:
     ap.add_argument("--eri-only", action="store_true", help="also time the class without J/K digestion")
     ap.add_argument("--once", action="store_true", help="launch each selected class once, no timing loop")
     ap.add_argument("--plan-only", action="store_true")
+    ap.add_argument("--onee", action="store_true", help="only build S, T, V once (the one-electron kernel)")
+    ap.add_argument("--jk-mixed", action="store_true",
+                    help="only run one mixed-precision J/K build of the workload's standard density")
     a = ap.parse_args(argv)
 
     mol, tau = workload(a.workload)
@@ -50,6 +54,18 @@ def main(argv=None) -> int:
     prof["plan_s"] = time.time() - t0
     prof["workload"] = a.workload
     print(json.dumps(prof), flush=True)
+    if a.onee or a.jk_mixed:
+        t0 = time.time()
+        if a.onee:
+            ctx.onee()
+        else:
+            # water clusters: 5 occupied orbitals per water, as cfg4
+            dens = (M.density_for(a.workload, mol) if a.workload in M.N_OCC
+                    else M.random_density(mol.n_sph, mol.n_sph * 5 // 24, seed=105))
+            ctx.jk(dens, mixed=True)
+        print(json.dumps({"onee" if a.onee else "jk_mixed": "done", "host_s": time.time() - t0}), flush=True)
+        ctx.close()
+        return 0
     want = {t.strip() for t in a.classes.split(",") if t.strip()}
     for i, c in enumerate(ctx.combos()):
         if want and tag(c) not in want:
