@@ -13,9 +13,12 @@ Printed JSON (one line, rank 0):
   jk_builds_per_s, fp64 {...}: builds/s and the plain-FP64 figures;
   accuracy       |dE| (E = tr(D (J - K/2))), max|dJ|, max|dK| of the mixed
                  build against the FP64 build on the last density;
-  roofline       dominant ERI kernel: algorithmic FP64 flops (flop model in
-                 origo_tlno_b200/csrc/plan.cpp) per launch / CUDA-event
-                 launch time, against the measured FP64 FMA peak;
+  roofline       dominant ERI kernel of the mixed step (the FP32 launch of
+                 the class that takes longest): algorithmic flops (flop
+                 model in origo_tlno_b200/csrc/plan.cpp) per launch /
+                 CUDA-event launch time, against the measured FP32 FMA peak;
+                 the FP64 launch of the same class beside it against the
+                 measured FP64 FMA peak;
   e2e            the same build through the host-buffer C-ABI call
                  (H2D of D, D2H of J and K inside the timed region);
   cpu_baseline   the reference engine (oracle/_ref, compiled from its
@@ -267,15 +270,20 @@ def _count_quartets(mol, tau):
 
 def _profiled_traffic(workload, tag):
     """DRAM bytes per launch of class `tag` on `workload` from the committed
-    ncu summary (profiles/dram_traffic.json), or None."""
+    ncu summary (profiles/dram_traffic.json): the FP32 kernel's entry
+    ("(10|00) fp32") when there is one, else the FP64 kernel's.  Returns
+    (bytes or None, which entry)."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         with open(path) as f:
             table = json.load(f)
     except (OSError, ValueError):
-        return None
-    v = table.get(workload, {}).get(tag)
-    return float(v) if v is not None else None
+        return None, None
+    for key in (tag + " fp32", tag):
+        v = table.get(workload, {}).get(key)
+        if v is not None:
+            return float(v), key
+    return None, None
 
 
 def _host_cpu():
@@ -565,20 +573,26 @@ def run_native(args):
     e2e = {"value": ws * quartets / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(Dh.nbytes),
            "d2h_bytes_per_step": int(out["J"].nbytes + out["K"].nbytes)}
 
-    # roofline of the dominant kernel (class combination with the largest time)
+    # Roofline of the dominant kernel of the timed (mixed) step: at the
+    # autotuned split most quartets run in the FP32 kernels, so the class
+    # whose FP32 launch over all its quartets takes longest is the dominant
+    # one; its FP64 launch is reported beside it.
     combos = ctx.combos()
     timings = []
     for i, cb in enumerate(combos):
         if cb["n_tiles"] == 0:
             continue
-        t = ctx.time_combo(i, fp32=False, reps=1)
+        t = ctx.time_combo(i, fp32=True, reps=1)
         timings.append((t, i, cb))
     timings.sort(key=lambda x: -x[0])
     tdom, idom, cdom = timings[0]
-    peak = E.fma_peak_tflops(False, device=local)
+    tdom64 = ctx.time_combo(idom, fp32=False, reps=1)
+    peak = E.fma_peak_tflops(True, device=local)
+    peak64 = E.fma_peak_tflops(False, device=local)
     achieved = cdom["flops"] / (tdom * 1e-3) / 1e12
+    achieved64 = cdom["flops"] / (tdom64 * 1e-3) / 1e12
     dom_tag = f"({cdom['la']}{cdom['lb']}|{cdom['lc']}{cdom['ld']})"
-    traffic = _profiled_traffic(args.config, dom_tag)
+    traffic, traffic_key = _profiled_traffic(args.config, dom_tag)
     # kernels per build: one per class combination and precision pass, the
     # max|D| reduction (mixed) and the two final symmetrisations
     n_cls = sum(1 for cb in combos if cb["n_tiles"] > 0)
@@ -628,15 +642,20 @@ def run_native(args):
                  "ms_per_step": 1e3 * t64 / steps},
         "mixed_speedup_vs_fp64": t64 / tmx,
         "accuracy": {"abs_dE_Eh": abs(dE), "max_abs_dJ": dJ, "max_abs_dK": dK},
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "kernel": f"eri_fast_jk_kernel<double> class {dom_tag}" if cdom["fast"] else
-                               f"eri_generic_jk_kernel<double> class {dom_tag}",
+                     "kernel": (f"eri_fast_jk_kernel<float> class {dom_tag}" if cdom["fast"] else
+                                f"eri_generic_cta_jk_kernel<float> class {dom_tag}") +
+                               " over all quartets of the class",
                      "launch_ms": tdom,
-                     "peak_source": "of measured: DFMA-chain probe (tlno_gpu_fma_peak) on this GPU; "
-                                    "MEASURED_PEAKS.json holds no FP64 figure",
-                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu "
-                                       "capture of the same class and workload (profiles/)"},
+                     "flops_per_launch_model": cdom["flops"],
+                     "peak_source": "of measured: FP32 FMA-chain probe (tlno_gpu_fma_peak) on this GPU; "
+                                    "MEASURED_PEAKS.json holds no FP32/FP64 CUDA-core figure",
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one ncu capture "
+                                       f"(profiles/dram_traffic.json entry {traffic_key!r} of {args.config})",
+                     "fp64": {"achieved": achieved64, "peak": peak64, "frac": achieved64 / peak64 if peak64 else None,
+                              "launch_ms": tdom64,
+                              "peak_source": "of measured: DFMA-chain probe (tlno_gpu_fma_peak) on this GPU"}},
         "e2e": e2e, "gpu_launches": launches * steps,
         "incremental": incremental, "eri_checksum_stream": checksum_leg, "one_electron": onee_leg,
         "clocks": clocks, "wall_s_timed": t_wall,

@@ -309,7 +309,10 @@ int tlno_gpu_batch_synchronize(tlno_gpu_batch* b);
 void* tlno_gpu_batch_stream(tlno_gpu_batch* b);
 
 /* Tuning of the kernel schedule: generic-kernel ket tile, generic warps
- * per CTA (0 = from the shared-memory budget), persistent grid multiplier
+ * per CTA (0 = the block-per-quartet generic kernel with the plan's pair
+ * projectors, or, for a plan too large to keep them, the warp-per-quartet
+ * kernel with warps from the shared-memory budget; 1..8 = the
+ * warp-per-quartet kernel with that many warps), persistent grid multiplier
  * (the compile-time kernels size their grid from the occupancy calculator,
  * capped by grid_mult x SMs), and streams (1..4): the class launches of a
  * build spread over that many streams (parallel branches of a captured

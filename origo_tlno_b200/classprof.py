@@ -45,11 +45,23 @@ def main(argv=None) -> int:
     ap.add_argument("--onee", action="store_true", help="only build S, T, V once (the one-electron kernel)")
     ap.add_argument("--jk-mixed", action="store_true",
                     help="only run one mixed-precision J/K build of the workload's standard density")
+    ap.add_argument("--force-generic", default="",
+                    help='comma-separated class tags run by the generic kernel even when compiled, such as "21|11"')
+    ap.add_argument("--generic-warps", type=int, default=0,
+                    help="0: block-per-quartet generic kernel; 1..8: warp-per-quartet kernel with that many warps")
     a = ap.parse_args(argv)
 
     mol, tau = workload(a.workload)
     t0 = time.time()
-    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=tau))
+    ctx = E.Context(mol)
+    for t in (t.strip() for t in a.force_generic.split(",")):
+        if t:
+            la, lb, lc, ld = int(t[0]), int(t[1]), int(t[3]), int(t[4])
+            X, Y = la * (la + 1) // 2 + lb, lc * (lc + 1) // 2 + ld
+            ctx.set_combo_generic(X * 15 + Y, True)
+    ctx.plan(E.ScreeningOptions(integral_threshold=tau))
+    if a.generic_warps:
+        ctx.set_tuning(generic_warps=a.generic_warps)
     prof = ctx.profile()
     prof["plan_s"] = time.time() - t0
     prof["workload"] = a.workload
@@ -58,6 +70,22 @@ def main(argv=None) -> int:
         t0 = time.time()
         if a.onee:
             ctx.onee()
+            if not a.once:
+                import torch
+                from . import _native as N
+                bufs = [torch.empty(mol.n_sph, mol.n_sph, dtype=torch.float64, device="cuda") for _ in range(3)]
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                st = torch.cuda.ExternalStream(ctx.stream())
+                ms = []
+                for _ in range(a.reps + 1):
+                    ev[0].record(st)
+                    N.check(N.lib().tlno_gpu_onee(ctx.h, bufs[0].data_ptr(), bufs[1].data_ptr(), bufs[2].data_ptr(),
+                                                  1, N.DEVICE_PTRS))
+                    ev[1].record(st)
+                    torch.cuda.synchronize()
+                    ms.append(ev[0].elapsed_time(ev[1]))
+                print(json.dumps({"onee_gpu_ms": min(ms[1:]), "M": mol.n_sph, "nuclei": int(len(mol.charges))}),
+                      flush=True)
         else:
             # water clusters: 5 occupied orbitals per water, as cfg4
             dens = (M.density_for(a.workload, mol) if a.workload in M.N_OCC

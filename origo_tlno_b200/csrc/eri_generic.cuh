@@ -404,5 +404,294 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// CTA-cooperative J/K kernel for the classes the compile-time kernels do not
+// cover (two f shells, or deep d/f slices).  One thread block works on one
+// contracted quartet at a time, so a class whose radial block, transfer
+// products and 2-D tables need tens of KB of shared memory keeps 4-8 warps
+// busy per block instead of one warp per block.  The HRR + spherical
+// projectors of both pairs come precomputed from the plan (one per shell
+// pair, built once per plan by pair_projector_kernel).
+//
+// Shared memory (doubles): region0 = max(NB item slots x 3 2-D tables,
+// X + V + the six density blocks), then the radial block T.
+struct GenericCtaLayout {
+    int las, lcs, ks, gs, nas, ncs, na, nb, nc, nd, nsab, nscd;
+    int nb_items;  // item slots per batch
+    int off_X, off_V, off_P, off_T, words;
+    __host__ __device__ void init(int la, int lb, int lc, int ld, int nbi) {
+        las = la + lb;
+        lcs = lc + ld;
+        ks = lcs + 1;
+        gs = (las + 1) * ks;
+        nas = ncart_cum(las) - cart_offset(la);
+        ncs = ncart_cum(lcs) - cart_offset(lc);
+        na = nsph(la); nb = nsph(lb); nc = nsph(lc); nd = nsph(ld);
+        nsab = na * nb;
+        nscd = nc * nd;
+        nb_items = nbi;
+        const int g_words = nb_items * 3 * gs;
+        off_X = 0;
+        off_V = off_X + nas * nscd;
+        off_P = off_V + nsab * nscd;
+        const int tail = off_P + na * nb + nc * nd + nb * nd + nb * nc + na * nd + na * nc;
+        off_T = ((g_words > tail ? g_words : tail) + 1) & ~1;
+        words = (off_T + nas * ncs + 1) & ~1;
+    }
+};
+
+// Projector block of one shell pair: Pm[s_ab * nslice + (flat(a') - off(la))].
+__device__ __forceinline__ int pair_projector_words(int la, int lb) {
+    return nsph(la) * nsph(lb) * (ncart_cum(la + lb) - cart_offset(la));
+}
+
+// Builds the projector of every pair that has an offset (warp per pair).
+__global__ void pair_projector_kernel(const int* pair_A, const int* pair_B, const double* shell_xyz,
+                                      const int* shell_L, const long long* off, int n_pairs, double* out) {
+    const int warps = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int k = blockIdx.x * warps + (threadIdx.x >> 5); k < n_pairs; k += gridDim.x * warps) {
+        const long long o = off[k];
+        if (o < 0) continue;
+        const int A = pair_A[k], B = pair_B[k];
+        const double* xa = shell_xyz + 3 * A;
+        const double* xb = shell_xyz + 3 * B;
+        build_pair_projector(out + o, shell_L[A], shell_L[B], xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2], lane);
+    }
+}
+
+template <typename R>
+__device__ void generic_quartet_cta(const PlanView& pv, const ClassLaunch& cl, const GenericCtaLayout& lay,
+                                    double* sm, int bra, int ket, bool jon, bool kon) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int A = pv.pair_A[bra], B = pv.pair_B[bra];
+    const int C = pv.pair_A[ket], D = pv.pair_B[ket];
+    const double* xa = pv.shell_xyz + 3 * A;
+    const double* xc = pv.shell_xyz + 3 * C;
+    const int la = cl.la, lb = cl.lb, lc = cl.lc, ld = cl.ld;
+    const int nroots = (la + lb + lc + ld) / 2 + 1;
+    const int npb = pv.pair_nprim[bra], npk = pv.pair_nprim[ket];
+    const int pob = pv.pair_prim_off[bra], pok = pv.pair_prim_off[ket];
+    const DPrimPair* pb = pv.prim + pob;
+    const DPrimPair* pk = pv.prim + pok;
+    R* Gs = reinterpret_cast<R*>(sm);
+    R* T = reinterpret_cast<R*>(sm + lay.off_T);
+    const int ntr = lay.nas * lay.ncs;
+    for (int e = tid; e < ntr; e += nt) T[e] = R(0);
+
+    const R Ax = R(xa[0]), Ay = R(xa[1]), Az = R(xa[2]);
+    const R Cx = R(xc[0]), Cy = R(xc[1]), Cz = R(xc[2]);
+    const int n_items = npb * npk * nroots;
+    const int gslot = 3 * lay.gs;
+    const int offa = cart_offset(la), offc = cart_offset(lc);
+    const bool fs_on = cl.fs_thr2 > 0.0 && la <= 3 && lb <= 3 && lc <= 3 && ld <= 3;
+    for (int base = 0; base < n_items; base += lay.nb_items) {
+        const int item = base + tid;
+        if (tid < lay.nb_items && item < n_items) {
+            const int r = item % nroots;
+            const int pq = item / nroots;
+            const int ib = pq / npk, ik = pq - ib * npk;
+            const DPrimPair bp = pb[ib];
+            const DPrimPair kp = pk[ik];
+            const R p = R(bp.p), q = R(kp.p);
+            const R pqs = p + q;
+            const R inv = R(1) / pqs;
+            const R PQx = R(bp.Px) - R(kp.Px), PQy = R(bp.Py) - R(kp.Py), PQz = R(bp.Pz) - R(kp.Pz);
+            const R Targ = p * q * inv * (PQx * PQx + PQy * PQy + PQz * PQz);
+            R t2, wt;
+            if (sizeof(R) == 4 && nroots >= 4) {
+                // FP64 carve-out of the FP32 pass: high-L roots and weights
+                double t2d, wtd;
+                rys_root<double>(nroots, double(Targ), r, t2d, wtd);
+                t2 = R(t2d);
+                wt = R(wtd);
+            } else {
+                rys_root<R>(nroots, Targ, r, t2, wt);
+            }
+            R pref = R(34.98683665524972497) * R(bp.w) * R(kp.w) / sqrt(pqs);
+            if (fs_on && !(pv.prim_fs[pob + ib] * pv.prim_fs[pok + ik] >= cl.fs_thr2)) pref = R(0);
+            const R qo = q * inv, po = p * inv;
+            const R b00 = R(0.5) * inv * t2;
+            const R b10 = R(0.5) * R(bp.invp) * (R(1) - qo * t2);
+            const R b01 = R(0.5) * R(kp.invp) * (R(1) - po * t2);
+            R* g = Gs + tid * gslot;
+            vrr_2d<R>(g, lay.las, lay.lcs, lay.ks, (R(bp.Px) - Ax) - qo * PQx * t2,
+                      (R(kp.Px) - Cx) + po * PQx * t2, b00, b10, b01, R(1));
+            vrr_2d<R>(g + lay.gs, lay.las, lay.lcs, lay.ks, (R(bp.Py) - Ay) - qo * PQy * t2,
+                      (R(kp.Py) - Cy) + po * PQy * t2, b00, b10, b01, R(1));
+            vrr_2d<R>(g + 2 * lay.gs, lay.las, lay.lcs, lay.ks, (R(bp.Pz) - Az) - qo * PQz * t2,
+                      (R(kp.Pz) - Cz) + po * PQz * t2, b00, b10, b01, pref * wt);
+        }
+        __syncthreads();
+        const int nvalid = min(lay.nb_items, n_items - base);
+        for (int e = tid; e < ntr; e += nt) {
+            const int ia = e / lay.ncs, ic = e - ia * lay.ncs;
+            const int fa = offa + ia, fc = offc + ic;
+            const int ix = c_cart.xyz[fa][0] * lay.ks + c_cart.xyz[fc][0];
+            const int iy = lay.gs + c_cart.xyz[fa][1] * lay.ks + c_cart.xyz[fc][1];
+            const int iz = 2 * lay.gs + c_cart.xyz[fa][2] * lay.ks + c_cart.xyz[fc][2];
+            R acc = T[e];
+            const R* g = Gs;
+            for (int s = 0; s < nvalid; ++s, g += gslot) acc += g[ix] * g[iy] * g[iz];
+            T[e] = acc;
+        }
+        __syncthreads();
+    }
+
+    // HRR + spherical projection with the plan's pair projectors:
+    // X = T PK^T, V = PB X.
+    const double* PB = pv.proj + pv.proj_off[bra];
+    const double* PK = pv.proj + pv.proj_off[ket];
+    double* X = sm + lay.off_X;
+    double* V = sm + lay.off_V;
+    for (int e = tid; e < lay.nas * lay.nscd; e += nt) {
+        const int ia = e / lay.nscd, s = e - ia * lay.nscd;
+        const R* trow = T + ia * lay.ncs;
+        const double* prow = PK + s * lay.ncs;
+        double acc = 0.0;
+        for (int ic = 0; ic < lay.ncs; ++ic) acc += double(trow[ic]) * __ldg(prow + ic);
+        X[e] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < lay.nsab * lay.nscd; e += nt) {
+        const int sab = e / lay.nscd, s = e - sab * lay.nscd;
+        const double* prow = PB + sab * lay.nas;
+        double acc = 0.0;
+        for (int ia = 0; ia < lay.nas; ++ia) acc += __ldg(prow + ia) * X[ia * lay.nscd + s];
+        V[e] = acc;
+    }
+    __syncthreads();
+
+    if (cl.checksum) {
+        // ERI checksum stream: canonical unique elements of the block
+        const int a0 = pv.shell_sph[A], b0 = pv.shell_sph[B];
+        const int c0 = pv.shell_sph[C], d0 = pv.shell_sph[D];
+        double s = 0.0;
+        for (int e = tid; e < lay.nsab * lay.nscd; e += nt) {
+            const int sab = e / lay.nscd, scd = e - sab * lay.nscd;
+            if (canonical_element(A == B, C == D, bra == ket, a0, sab / lay.nb, b0, sab % lay.nb, c0,
+                                  scd / lay.nd, d0, scd % lay.nd))
+                s += V[e];
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((tid & 31) == 0 && s != 0.0) atomicAdd(cl.checksum, s);
+        __syncthreads();
+        return;
+    }
+    // J/K digestion with shell-level degeneracy f (consumer_policies.ipp:87-157)
+    const int mol = pv.pair_mol ? pv.pair_mol[bra] : 0;
+    const int M = pv.mol_M ? pv.mol_M[mol] : cl.M;
+    const long long mbase = pv.mol_mat_off ? pv.mol_mat_off[mol] : 0;
+    const double* Dm = cl.dens + mbase;
+    double* Jm = cl.J + mbase;
+    double* Km = cl.K + mbase;
+    const int a0 = pv.shell_sph[A], b0 = pv.shell_sph[B];
+    const int c0 = pv.shell_sph[C], d0 = pv.shell_sph[D];
+    double f = 1.0;
+    if (A == B) f *= 0.5;
+    if (C == D) f *= 0.5;
+    if (bra == ket) f *= 0.5;
+    const int na = lay.na, nb = lay.nb, nc = lay.nc, nd = lay.nd;
+    double* Pab = sm + lay.off_P;
+    double* Pcd = Pab + na * nb;
+    double* Pbd = Pcd + nc * nd;
+    double* Pbc = Pbd + nb * nd;
+    double* Pad = Pbc + nb * nc;
+    double* Pac = Pad + na * nd;
+    for (int e = tid; e < na * nb; e += nt) Pab[e] = Dm[(long long)(a0 + e / nb) * M + b0 + e % nb];
+    for (int e = tid; e < nc * nd; e += nt) Pcd[e] = Dm[(long long)(c0 + e / nd) * M + d0 + e % nd];
+    for (int e = tid; e < nb * nd; e += nt) Pbd[e] = Dm[(long long)(b0 + e / nd) * M + d0 + e % nd];
+    for (int e = tid; e < nb * nc; e += nt) Pbc[e] = Dm[(long long)(b0 + e / nc) * M + c0 + e % nc];
+    for (int e = tid; e < na * nd; e += nt) Pad[e] = Dm[(long long)(a0 + e / nd) * M + d0 + e % nd];
+    for (int e = tid; e < na * nc; e += nt) Pac[e] = Dm[(long long)(a0 + e / nc) * M + c0 + e % nc];
+    __syncthreads();
+    const int nscd = lay.nscd;
+    if (cl.want_j && jon) {
+        const double fj = 4.0 * f;
+        for (int sab = tid; sab < na * nb; sab += nt) {
+            double s = 0.0;
+            for (int t = 0; t < nscd; ++t) s += V[sab * nscd + t] * Pcd[t];
+            atomicAdd(Jm + (long long)(a0 + sab / nb) * M + b0 + sab % nb, fj * s);
+        }
+        for (int scd = tid; scd < nscd; scd += nt) {
+            double s = 0.0;
+            for (int t = 0; t < na * nb; ++t) s += V[t * nscd + scd] * Pab[t];
+            atomicAdd(Jm + (long long)(c0 + scd / nd) * M + d0 + scd % nd, fj * s);
+        }
+    }
+    if (cl.want_k && kon) {
+        const double fk = 2.0 * f;
+        const int nac = na * nc, nad = na * nd, nbc = nb * nc, nbd = nb * nd;
+        for (int e = tid; e < nac + nad + nbc + nbd; e += nt) {
+            double s = 0.0;
+            if (e < nac) {
+                const int a = e / nc, c = e % nc;
+                for (int b = 0; b < nb; ++b)
+                    for (int d = 0; d < nd; ++d) s += V[(a * nb + b) * nscd + c * nd + d] * Pbd[b * nd + d];
+                atomicAdd(Km + (long long)(a0 + a) * M + c0 + c, fk * s);
+            } else if (e < nac + nad) {
+                const int k = e - nac, a = k / nd, d = k % nd;
+                for (int b = 0; b < nb; ++b)
+                    for (int c = 0; c < nc; ++c) s += V[(a * nb + b) * nscd + c * nd + d] * Pbc[b * nc + c];
+                atomicAdd(Km + (long long)(a0 + a) * M + d0 + d, fk * s);
+            } else if (e < nac + nad + nbc) {
+                const int k = e - nac - nad, b = k / nc, c = k % nc;
+                for (int a = 0; a < na; ++a)
+                    for (int d = 0; d < nd; ++d) s += V[(a * nb + b) * nscd + c * nd + d] * Pad[a * nd + d];
+                atomicAdd(Km + (long long)(b0 + b) * M + c0 + c, fk * s);
+            } else {
+                const int k = e - nac - nad - nbc, b = k / nd, d = k % nd;
+                for (int a = 0; a < na; ++a)
+                    for (int c = 0; c < nc; ++c) s += V[(a * nb + b) * nscd + c * nd + d] * Pac[a * nc + c];
+                atomicAdd(Km + (long long)(b0 + b) * M + d0 + d, fk * s);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Tiled schedule (J/K mode), one quartet per block at a time: tile = 1 bra
+// pair x bk ket pairs, tiles handed out by a block-wide dynamic counter.
+template <typename R>
+__global__ void eri_generic_cta_jk_kernel(PlanView pv, ClassLaunch cl, int nb_items) {
+    extern __shared__ double smem[];
+    GenericCtaLayout lay;
+    lay.init(cl.la, cl.lb, cl.lc, cl.ld, nb_items);
+    __shared__ int s_tile;
+    const double thr = (cl.prec_mode != 0) ? cl.tau_mix / fmax(*cl.dmax, 1e-300) : 0.0;
+    const int ntiles = cl.tile_end - cl.tile_begin;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(cl.counter, 1);
+        __syncthreads();
+        const int t = s_tile;
+        __syncthreads();
+        if (t >= ntiles) break;
+        const int tile = cl.tile_begin + t;
+        const int b = find_block(cl.tile_prefix, cl.n_blocks, tile);
+        const int kb = tile - __ldg(cl.tile_prefix + b);
+        const BlockDesc bd = cl.blocks[b];
+        const int bra = __ldg(cl.bra_list + bd.bra0);  // one bra per block
+        const int i = bra - bd.xbeg;
+        const double qi = pv.pair_Q[bra];
+        for (int jj = 0; jj < cl.bk; ++jj) {
+            const int j = kb * cl.bk + jj;
+            if (j >= bd.nket) break;
+            if (cl.same && bd.koff + j > i) break;
+            const int ket = bd.ket0 + j;
+            const double qq = qi * pv.pair_Q[ket];
+            if (!(qq >= cl.tau)) continue;
+            if (cl.prec_mode == 1 && !(qq >= thr)) continue;
+            if (cl.prec_mode == 2 && qq >= thr) continue;
+            bool lj = true, lk = true;
+            if (cl.den.mode) {
+                const int mol = pv.pair_mol ? pv.pair_mol[ket] : 0;
+                density_live(cl, pv, mol, pv.pair_A[bra], pv.pair_B[bra], pv.pair_A[ket], pv.pair_B[ket], qq, lj, lk);
+                if (!lj && !lk) continue;
+            }
+            generic_quartet_cta<R>(pv, cl, lay, smem, bra, ket, lj, lk);
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace tlno_gpu

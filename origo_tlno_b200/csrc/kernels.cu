@@ -442,6 +442,9 @@ void ensure_device_tables() {
     TLNO_CUDA(cudaFuncSetAttribute(eri_generic_list_kernel<double, kSchwarz>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
     TLNO_CUDA(cudaFuncSetAttribute(eri_generic_jk_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
     TLNO_CUDA(cudaFuncSetAttribute(eri_generic_jk_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    // (the block-per-quartet kernel also holds a little static shared memory)
+    TLNO_CUDA(cudaFuncSetAttribute(eri_generic_cta_jk_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm - 1024));
+    TLNO_CUDA(cudaFuncSetAttribute(eri_generic_cta_jk_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm - 1024));
     done.insert(devid);
 }
 
@@ -476,9 +479,52 @@ void launch_eri_schwarz(const PlanView& pv, const ClassLaunch& cl, cudaStream_t 
     TLNO_CUDA(cudaGetLastError());
 }
 
+void launch_pair_projectors(const int* pair_A, const int* pair_B, const double* shell_xyz, const int* shell_L,
+                            const long long* off, int n_pairs, double* out, cudaStream_t s) {
+    if (n_pairs == 0) return;
+    const int warps = 8;
+    const int grid = std::min((n_pairs + warps - 1) / warps, sm_count() * 16);
+    pair_projector_kernel<<<grid, 32 * warps, 0, s>>>(pair_A, pair_B, shell_xyz, shell_L, off, n_pairs, out);
+    TLNO_CUDA(cudaGetLastError());
+}
+
+// CTA shape of the generic J/K kernel for a class: threads per block and item
+// slots per batch, and the dynamic shared memory it needs.
+static void generic_cta_shape(int la, int lb, int lc, int ld, int& threads, int& nb_items, int& bytes) {
+    GenericCtaLayout lay;
+    lay.init(la, lb, lc, ld, 1);
+    threads = lay.nas * lay.ncs > 2048 ? 256 : 128;
+    nb_items = 64;
+    for (;;) {
+        lay.init(la, lb, lc, ld, nb_items);
+        if (lay.words * 8 <= 100 * 1024 || nb_items <= 16) break;
+        nb_items /= 2;
+    }
+    bytes = lay.words * 8;
+}
+
 void launch_eri_jk_generic(const PlanView& pv, const ClassLaunch& cl, bool fp32, int warps, int grid,
                            cudaStream_t s) {
     if (cl.tile_end <= cl.tile_begin) return;
+    if (pv.proj && warps <= 0) {
+        // one quartet per block at a time, projectors from the plan
+        int threads = 0, nb_items = 0, bytes = 0;
+        generic_cta_shape(cl.la, cl.lb, cl.lc, cl.ld, threads, nb_items, bytes);
+        int per_sm = 0;
+        if (fp32) {
+            TLNO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eri_generic_cta_jk_kernel<float>, threads, bytes));
+        } else {
+            TLNO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eri_generic_cta_jk_kernel<double>, threads, bytes));
+        }
+        const int ntiles = cl.tile_end - cl.tile_begin;
+        const int g = std::max(1, std::min(ntiles, sm_count() * std::max(per_sm, 1)));
+        if (fp32)
+            eri_generic_cta_jk_kernel<float><<<g, threads, bytes, s>>>(pv, cl, nb_items);
+        else
+            eri_generic_cta_jk_kernel<double><<<g, threads, bytes, s>>>(pv, cl, nb_items);
+        TLNO_CUDA(cudaGetLastError());
+        return;
+    }
     const int bytes = generic_warp_bytes(cl.la, cl.lb, cl.lc, cl.ld);
     if (warps <= 0) warps = generic_warps_for(bytes);
     while (warps > 1 && bytes * warps > 200 * 1024) --warps;
@@ -539,8 +585,10 @@ bool launch_eri_jk_fast(const PlanView& pv, const ClassLaunch& cl, bool fp32, in
 void launch_onee(const OneeLaunch& L, cudaStream_t s) {
     if (L.n_pairs == 0) return;
     const int warps = 4;
+    const int smem = warps * kOneeWarpWords * static_cast<int>(sizeof(double));
+    TLNO_CUDA(cudaFuncSetAttribute(onee_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min((L.n_pairs + warps - 1) / warps, sm_count() * 16);
-    onee_kernel<<<grid, 32 * warps, 0, s>>>(L);
+    onee_kernel<<<grid, 32 * warps, smem, s>>>(L);
     TLNO_CUDA(cudaGetLastError());
 }
 

@@ -17,6 +17,9 @@ void ensure_device_tables();
 
 // Shared-memory bytes per warp of the generic kernel for a class.
 int generic_warp_bytes(int la, int lb, int lc, int ld);
+// Builds the pair projectors of every pair with an offset >= 0.
+void launch_pair_projectors(const int* pair_A, const int* pair_B, const double* shell_xyz, const int* shell_L,
+                            const long long* off, int n_pairs, double* out, cudaStream_t s);
 
 void launch_eri_store(const dev::PlanView& pv, const dev::ClassLaunch& cl, cudaStream_t s);
 void launch_eri_schwarz(const dev::PlanView& pv, const dev::ClassLaunch& cl, cudaStream_t s);

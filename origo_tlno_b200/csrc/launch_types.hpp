@@ -39,6 +39,11 @@ struct PlanView {
     // indexed by molecule-local shells); null for a single molecule.
     const int* mol_shell_off;
     const int* mol_ns;
+    // HRR + spherical projector of each pair used by a generic class
+    // combination: proj + proj_off[pair], rows s_ab of ncart slices
+    // |a'| in [La, La+Lb]; null when the plan keeps none.
+    const double* proj;
+    const long long* proj_off;
 };
 
 // Density (CVHF) screen of one build (direct_build.ipp:122-251,

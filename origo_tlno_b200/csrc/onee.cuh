@@ -1,16 +1,19 @@
 // One-electron overlap, kinetic and nuclear-attraction integrals.
 //
-// One warp per screened shell pair (A, B), L_A >= L_B:
+// One warp per screened shell pair (A, B), L_A >= L_B, with its Cartesian
+// S, T, V blocks in shared memory:
 //  * S and T: each lane owns Cartesian component pairs and walks the
 //    primitive pairs with the Obara-Saika 1-D shape tables extended to
 //    l_b + 2, kinetic 1-D factor
 //    T_x = b(2l_b+1) S(l_a,l_b) - 2b^2 S(l_a,l_b+2) - l_b(l_b-1)/2 S(l_a,l_b-2)
 //    (reference: integrals/one_electron/onee_integrals.cpp:32-51, 284-416);
-//  * V: each lane owns a strided subset of the nuclei; per primitive pair it
-//    forms the Boys seeds (-2p)^n F_n(p |P-C|^2), the McMurchie-Davidson
-//    R_tuv recursion, sums Z_K R_tuv over its nuclei and contracts with the
-//    Hermite expansion coefficients E^t_ij (onee_integrals.cpp:53-157,
-//    477-887); lane partials are reduced at the end;
+//  * V: per primitive pair each lane takes a strided subset of the nuclei,
+//    forms the Boys seeds (-2p)^n F_n(p |P-C|^2) and the McMurchie-Davidson
+//    R_tuv recursion (unrolled per total order, in registers) and sums
+//    Z_K R_tuv; the warp reduces the sums once, three lanes build the
+//    Hermite expansion coefficients E^t_ij of the three axes, and the lanes,
+//    now owning component pairs, contract them (onee_integrals.cpp:53-157,
+//    477-887);
 //  * the Cartesian blocks are transformed to real spherical harmonics and
 //    written to both triangles of the M x M outputs
 //    (onee_matrices.cpp:226-309, 554-607).
@@ -119,9 +122,114 @@ __device__ __forceinline__ void boys_seeds(int maxn, double x, double p, double*
     }
 }
 
-__global__ void onee_kernel(OneeLaunch L) {
+// Per-warp shared memory of the one-electron kernel (doubles): the Cartesian
+// S, T, V blocks, the nucleus-summed R_tuv and the three Hermite tables.
+constexpr int kOneeBlk = kOneeMaxCart * kOneeMaxCart;
+constexpr int kOneeEAxis = (kMaxL + 1) * (kMaxL + 1) * (2 * kMaxL + 1);
+constexpr int kOneeWarpWords = 3 * kOneeBlk + kNCartCum8 + 3 * kOneeEAxis + 1;  // 16-byte multiple
+
+// sum_K Z_K R^{(0)}_{tuv}(P - C_K) over this lane's nuclei for total order LT
+// (compile-time, in registers), reduced over the warp into
+// Rw[cart_flat(t, u, v)].  Downward recursion in n of
+// R^{(n)}_{t,u,v} = X R^{(n+1)}_{t-1,u,v} + (t-1) R^{(n+1)}_{t-2,u,v} (and the
+// same in u, v), seeded by R^{(n)}_{000} = (-2p)^n F_n(p |P-C|^2)
+// (onee_integrals.cpp:108-157), done in place: within a level the orders are
+// visited from the highest down, so every entry of the next level is read
+// before it is overwritten.
+template <int LT>
+__device__ __forceinline__ void nuclear_r_sum(const OneeLaunch& L, double Px, double Py, double Pz, double p,
+                                              int lane, double* Rw) {
+    constexpr int NR = (LT + 1) * (LT + 2) * (LT + 3) / 6;
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    for (int K = lane; K < L.n_nuc; K += 32) {
+        const double cx = Px - L.nuc[4 * K], cy = Py - L.nuc[4 * K + 1], cz = Pz - L.nuc[4 * K + 2];
+        const double Zk = L.nuc[4 * K + 3];
+        double F[LT + 1];
+        boys_seeds(LT, p * (cx * cx + cy * cy + cz * cz), p, F);
+        double R[NR];
+        R[0] = F[LT];
+#pragma unroll
+        for (int n = LT - 1; n >= 0; --n) {
+#pragma unroll
+            for (int tot = LT - n; tot >= 1; --tot) {
+#pragma unroll
+                for (int t = tot; t >= 0; --t) {
+#pragma unroll
+                    for (int u = tot - t; u >= 0; --u) {
+                        const int v = tot - t - u;
+                        double val;
+                        if (t > 0)
+                            val = cx * R[cart_flat(t - 1, u, v)] + (t > 1 ? (t - 1) * R[cart_flat(t - 2, u, v)] : 0.0);
+                        else if (u > 0)
+                            val = cy * R[cart_flat(t, u - 1, v)] + (u > 1 ? (u - 1) * R[cart_flat(t, u - 2, v)] : 0.0);
+                        else
+                            val = cz * R[cart_flat(t, u, v - 1)] + (v > 1 ? (v - 1) * R[cart_flat(t, u, v - 2)] : 0.0);
+                        R[cart_flat(t, u, v)] = val;
+                    }
+                }
+            }
+            R[0] = F[n];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] += Zk * R[r];
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        double v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) Rw[r] = v;
+    }
+}
+
+// The same for total orders above 4 (pairs with f or g shells), with the
+// recursion levels in per-thread arrays.
+__device__ __noinline__ void nuclear_r_sum_any(const OneeLaunch& L, int ltot, double Px, double Py, double Pz,
+                                               double p, int lane, double* Rw) {
+    const int nR = ncart_cum(ltot);
+    double Rs[kNCartCum8], R0[kNCartCum8], R1[kNCartCum8];
+    double F[2 * kMaxL + 1];
+    for (int r = 0; r < nR; ++r) Rs[r] = 0.0;
+    for (int K = lane; K < L.n_nuc; K += 32) {
+        const double cx = Px - L.nuc[4 * K], cy = Py - L.nuc[4 * K + 1], cz = Pz - L.nuc[4 * K + 2];
+        const double Zk = L.nuc[4 * K + 3];
+        boys_seeds(ltot, p * (cx * cx + cy * cy + cz * cz), p, F);
+        double* cur = R0;
+        double* nxt = R1;
+        for (int n = ltot; n >= 0; --n) {
+            const int lim = ltot - n;
+            cur[0] = F[n];
+            for (int tot = 1; tot <= lim; ++tot)
+                for (int t = tot; t >= 0; --t)
+                    for (int u = tot - t; u >= 0; --u) {
+                        const int v = tot - t - u;
+                        double val;
+                        if (t > 0) val = cx * nxt[cart_flat(t - 1, u, v)] + (t > 1 ? (t - 1) * nxt[cart_flat(t - 2, u, v)] : 0.0);
+                        else if (u > 0) val = cy * nxt[cart_flat(t, u - 1, v)] + (u > 1 ? (u - 1) * nxt[cart_flat(t, u - 2, v)] : 0.0);
+                        else val = cz * nxt[cart_flat(t, u, v - 1)] + (v > 1 ? (v - 1) * nxt[cart_flat(t, u, v - 2)] : 0.0);
+                        cur[cart_flat(t, u, v)] = val;
+                    }
+            double* tmp = cur; cur = nxt; nxt = tmp;
+        }
+        for (int r = 0; r < nR; ++r) Rs[r] += Zk * nxt[r];
+    }
+    for (int r = 0; r < nR; ++r) {
+        double v = Rs[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) Rw[r] = v;
+    }
+}
+
+__global__ void __launch_bounds__(128) onee_kernel(OneeLaunch L) {
+    extern __shared__ double onee_smem[];
     const int warps = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* Sc = onee_smem + warp * kOneeWarpWords;  // Cartesian S block [ca * ncb + cb]
+    double* Tc = Sc + kOneeBlk;
+    double* Vc = Tc + kOneeBlk;
+    double* Rw = Vc + kOneeBlk;                       // nucleus-summed R_tuv
+    double* Ew = Rw + kNCartCum8;                     // Hermite tables, one per axis
     for (int pi = blockIdx.x * warps + warp; pi < L.n_pairs; pi += gridDim.x * warps) {
         const OneePair pr = L.pairs[pi];
         const int A = pr.A, B = pr.B;
@@ -134,14 +242,15 @@ __global__ void onee_kernel(OneeLaunch L) {
         const int npa = L.shell_nprim[A], npb = L.shell_nprim[B];
         const int pa0 = L.shell_prim[A], pb0 = L.shell_prim[B];
         const int offa = cart_offset(la), offb = cart_offset(lb);
-
-        double sblk[8], tblk[8], vblk[kOneeMaxCart * kOneeMaxCart];
-        // ---- overlap and kinetic: lanes own component pairs ----
         const int ncomp = nca * ncb;
-        for (int k = 0; k < 8; ++k) { sblk[k] = 0.0; tblk[k] = 0.0; }
+        for (int cc = lane; cc < ncomp; cc += 32) {
+            Sc[cc] = 0.0;
+            Tc[cc] = 0.0;
+            Vc[cc] = 0.0;
+        }
+        // ---- overlap and kinetic: lanes own component pairs ----
         if (pr.do_st) {
-            int slot = 0;
-            for (int cc = lane; cc < ncomp; cc += 32, ++slot) {
+            for (int cc = lane; cc < ncomp; cc += 32) {
                 const int ca = cc / ncb, cb = cc % ncb;
                 const int ax = c_cart.xyz[offa + ca][0], ay = c_cart.xyz[offa + ca][1], az = c_cart.xyz[offa + ca][2];
                 const int bx = c_cart.xyz[offb + cb][0], by = c_cart.xyz[offb + cb][1], bz = c_cart.xyz[offb + cb][2];
@@ -186,21 +295,15 @@ __global__ void onee_kernel(OneeLaunch L) {
                         t_acc += w * (tx * sy * sz + sx * ty * sz + sx * sy * tz);
                     }
                 }
-                sblk[slot] = s_acc;
-                tblk[slot] = t_acc;
+                Sc[cc] = s_acc;
+                Tc[cc] = t_acc;
             }
         }
-        // ---- nuclear attraction: lanes own nuclei ----
-        for (int k = 0; k < ncomp; ++k) vblk[k] = 0.0;
+        // ---- nuclear attraction: lanes own nuclei, then component pairs ----
         if (pr.do_v) {
             const int ltot = la + lb;
             const int nt = ltot + 1, col = lb + 1;
-            const int nR = ncart_cum(ltot);
-            double Ex[(kMaxL + 1) * (kMaxL + 1) * (2 * kMaxL + 1)];
-            double Ey[(kMaxL + 1) * (kMaxL + 1) * (2 * kMaxL + 1)];
-            double Ez[(kMaxL + 1) * (kMaxL + 1) * (2 * kMaxL + 1)];
-            double Rs[kNCartCum8], R0[kNCartCum8], R1[kNCartCum8];
-            double F[2 * kMaxL + 1];
+            double v00 = 0.0;  // s-s: this lane's share
             for (int ia = 0; ia < npa; ++ia) {
                 const double alpha = L.exps[pa0 + ia];
                 for (int ib = 0; ib < npb; ++ib) {
@@ -221,90 +324,56 @@ __global__ void onee_kernel(OneeLaunch L) {
                         double nuc_sum = 0.0;
                         for (int K = lane; K < L.n_nuc; K += 32) {
                             const double cx = Px - L.nuc[4 * K], cy = Py - L.nuc[4 * K + 1], cz = Pz - L.nuc[4 * K + 2];
-                            boys_seeds(0, p * (cx * cx + cy * cy + cz * cz), p, F);
-                            nuc_sum += L.nuc[4 * K + 3] * F[0];
+                            double F0[1];
+                            boys_seeds(0, p * (cx * cx + cy * cy + cz * cz), p, F0);
+                            nuc_sum += L.nuc[4 * K + 3] * F0[0];
                         }
-                        const double vprim = neg2pi_over_p * emc * nuc_sum;
-                        vblk[0] += L.comp_coef[L.comp_off[A] + ia] * L.comp_coef[L.comp_off[B] + ib] * vprim;
+                        v00 += L.comp_coef[L.comp_off[A] + ia] * L.comp_coef[L.comp_off[B] + ib] *
+                               (neg2pi_over_p * emc * nuc_sum);
                         continue;
                     }
-                    for (int r = 0; r < nR; ++r) Rs[r] = 0.0;
-                    bool any = false;
-                    for (int K = lane; K < L.n_nuc; K += 32) {
-                        const double cx = Px - L.nuc[4 * K], cy = Py - L.nuc[4 * K + 1], cz = Pz - L.nuc[4 * K + 2];
-                        const double Zk = L.nuc[4 * K + 3];
-                        boys_seeds(ltot, p * (cx * cx + cy * cy + cz * cz), p, F);
-                        // R^{(n)}_{tuv} from n = ltot down to 0, two compact levels
-                        double* cur = R0;
-                        double* nxt = R1;
-                        for (int n = ltot; n >= 0; --n) {
-                            const int lim = ltot - n;
-                            cur[0] = F[n];
-                            for (int tot = 1; tot <= lim; ++tot) {
-                                for (int t = tot; t >= 0; --t)
-                                    for (int u = tot - t; u >= 0; --u) {
-                                        const int v = tot - t - u;
-                                        const int idx = cart_flat(t, u, v);
-                                        double val;
-                                        if (t > 0) val = cx * nxt[cart_flat(t - 1, u, v)] + (t > 1 ? (t - 1) * nxt[cart_flat(t - 2, u, v)] : 0.0);
-                                        else if (u > 0) val = cy * nxt[cart_flat(t, u - 1, v)] + (u > 1 ? (u - 1) * nxt[cart_flat(t, u - 2, v)] : 0.0);
-                                        else val = cz * nxt[cart_flat(t, u, v - 1)] + (v > 1 ? (v - 1) * nxt[cart_flat(t, u, v - 2)] : 0.0);
-                                        cur[idx] = val;
-                                    }
-                            }
-                            double* tmp = cur; cur = nxt; nxt = tmp;
-                        }
-                        // the last level written (n = 0) is in nxt
-                        for (int r = 0; r < nR; ++r) Rs[r] += Zk * nxt[r];
-                        any = true;
+                    __syncwarp();  // the previous primitive pair's readers are done
+                    switch (ltot) {
+                        case 1: nuclear_r_sum<1>(L, Px, Py, Pz, p, lane, Rw); break;
+                        case 2: nuclear_r_sum<2>(L, Px, Py, Pz, p, lane, Rw); break;
+                        case 3: nuclear_r_sum<3>(L, Px, Py, Pz, p, lane, Rw); break;
+                        case 4: nuclear_r_sum<4>(L, Px, Py, Pz, p, lane, Rw); break;
+                        default: nuclear_r_sum_any(L, ltot, Px, Py, Pz, p, lane, Rw); break;
                     }
-                    if (!any) continue;
                     const double inv2p = 0.5 * invp;
-                    hermite_table(Ex, la, lb, ab[0], alpha, beta, inv2p, exp(-chi * ab[0] * ab[0]));
-                    hermite_table(Ey, la, lb, ab[1], alpha, beta, inv2p, exp(-chi * ab[1] * ab[1]));
-                    hermite_table(Ez, la, lb, ab[2], alpha, beta, inv2p, exp(-chi * ab[2] * ab[2]));
-                    for (int ca = 0; ca < nca; ++ca) {
+                    if (lane < 3)
+                        hermite_table(Ew + lane * kOneeEAxis, la, lb, ab[lane], alpha, beta, inv2p,
+                                      exp(-chi * ab[lane] * ab[lane]));
+                    __syncwarp();
+                    for (int cc = lane; cc < ncomp; cc += 32) {
+                        const int ca = cc / ncb, cb = cc % ncb;
                         const int ax = c_cart.xyz[offa + ca][0], ay = c_cart.xyz[offa + ca][1], az = c_cart.xyz[offa + ca][2];
+                        const int bx = c_cart.xyz[offb + cb][0], by = c_cart.xyz[offb + cb][1], bz = c_cart.xyz[offb + cb][2];
                         const double da = L.comp_coef[L.comp_off[A] + ca * npa + ia];
-                        for (int cb = 0; cb < ncb; ++cb) {
-                            const int bx = c_cart.xyz[offb + cb][0], by = c_cart.xyz[offb + cb][1], bz = c_cart.xyz[offb + cb][2];
-                            const double db = L.comp_coef[L.comp_off[B] + cb * npb + ib];
-                            const double* ex = Ex + (ax * col + bx) * nt;
-                            const double* ey = Ey + (ay * col + by) * nt;
-                            const double* ez = Ez + (az * col + bz) * nt;
-                            double s = 0.0;
-                            for (int t = 0; t <= ax + bx; ++t)
-                                for (int u = 0; u <= ay + by; ++u) {
-                                    const double exy = ex[t] * ey[u];
-                                    for (int v = 0; v <= az + bz; ++v) s += exy * ez[v] * Rs[cart_flat(t, u, v)];
-                                }
-                            vblk[ca * ncb + cb] += (da * db * neg2pi_over_p) * s;
-                        }
+                        const double db = L.comp_coef[L.comp_off[B] + cb * npb + ib];
+                        const double* ex = Ew + (ax * col + bx) * nt;
+                        const double* ey = Ew + kOneeEAxis + (ay * col + by) * nt;
+                        const double* ez = Ew + 2 * kOneeEAxis + (az * col + bz) * nt;
+                        double s = 0.0;
+                        for (int t = 0; t <= ax + bx; ++t)
+                            for (int u = 0; u <= ay + by; ++u) {
+                                const double exy = ex[t] * ey[u];
+                                for (int v = 0; v <= az + bz; ++v) s += exy * ez[v] * Rw[cart_flat(t, u, v)];
+                            }
+                        Vc[cc] += (da * db * neg2pi_over_p) * s;
                     }
                 }
             }
-            for (int k = 0; k < ncomp; ++k) {
-                double v = vblk[k];
-                for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                vblk[k] = v;
+            if (ltot == 0) {
+                for (int o = 16; o > 0; o >>= 1) v00 += __shfl_xor_sync(0xffffffffu, v00, o);
+                if (lane == 0) Vc[0] = v00;
             }
         }
+        __syncwarp();
         // ---- spherical transform and scatter ----
-        // Gather S/T blocks from the owning lanes through shuffles.
         const int nsa = nsph(la), nsb = nsph(lb);
         const int a0 = L.shell_sph[A], b0 = L.shell_sph[B];
         const int M = L.M;
-        double s_full[kOneeMaxCart * kOneeMaxCart], t_full[kOneeMaxCart * kOneeMaxCart];
-        if (pr.do_st) {
-            for (int cc = 0; cc < ncomp; ++cc) {
-                const int owner = cc & 31, slot = cc >> 5;
-                double sv = 0.0, tv = 0.0;
-                // every lane contributes its slot value; select the owner's
-                for (int k = 0; k < 8; ++k) if (k == slot) { sv = sblk[k]; tv = tblk[k]; }
-                s_full[cc] = __shfl_sync(0xffffffffu, sv, owner);
-                t_full[cc] = __shfl_sync(0xffffffffu, tv, owner);
-            }
-        }
         for (int e = lane; e < nsa * nsb; e += 32) {
             const int sa = e / nsb, sb = e % nsb;
             double sv = 0.0, tv = 0.0, vv = 0.0;
@@ -316,8 +385,9 @@ __global__ void onee_kernel(OneeLaunch L) {
                     if (c_c2s.sph[eb] != sb) continue;
                     const double k = ka * c_c2s.coef_raw[eb];
                     const int idx = ca * ncb + c_c2s.cart[eb];
-                    if (pr.do_st) { sv += k * s_full[idx]; tv += k * t_full[idx]; }
-                    if (pr.do_v) vv += k * vblk[idx];
+                    sv += k * Sc[idx];
+                    tv += k * Tc[idx];
+                    vv += k * Vc[idx];
                 }
             }
             const long long ij = (long long)(a0 + sa) * M + b0 + sb;
@@ -325,6 +395,7 @@ __global__ void onee_kernel(OneeLaunch L) {
             if (pr.do_st) { L.S[ij] = sv; L.S[ji] = sv; L.T[ij] = tv; L.T[ji] = tv; }
             if (pr.do_v) { L.V[ij] = vv; L.V[ji] = vv; }
         }
+        __syncwarp();
     }
 }
 

@@ -333,6 +333,8 @@ dev::PlanView Plan2e::view() const {
     pv.prim_fs = d_prim_fs.as<double>();
     pv.mol_shell_off = n_mol > 1 ? d_mol_shell_off.as<int>() : nullptr;
     pv.mol_ns = n_mol > 1 ? d_mol_ns.as<int>() : nullptr;
+    pv.proj = proj_ready ? d_proj.as<double>() : nullptr;
+    pv.proj_off = proj_ready ? d_proj_off.as<long long>() : nullptr;
     return pv;
 }
 
@@ -604,6 +606,34 @@ void build_plan(Plan2e& plan, const std::vector<const Basis*>& bases, std::vecto
         }
     }
     plan.d_counters.alloc(sizeof(int) * 2 * std::max<std::size_t>(plan.combos.size(), 1));
+
+    // HRR + spherical projectors of the pairs of every pair class that a
+    // generic (CTA) class combination uses, built once on the device.
+    {
+        std::array<bool, kMaxPairClasses> need{};
+        for (const ComboSchedule& cs : plan.combos)
+            if (!cs.fast) need[cs.X] = need[cs.Y] = true;
+        const std::size_t np = plan.pair_A.size();
+        plan.proj_off.assign(np, -1);
+        long long words = 0;
+        for (std::size_t k = 0; k < np; ++k) {
+            const int la = Ls[plan.pair_A[k]], lb = Ls[plan.pair_B[k]];
+            if (!need[la * (la + 1) / 2 + lb]) continue;
+            plan.proj_off[k] = words;
+            const int nslice = (la + lb + 1) * (la + lb + 2) * (la + lb + 3) / 6 - la * (la + 1) * (la + 2) / 6;
+            words += static_cast<long long>(2 * la + 1) * (2 * lb + 1) * nslice;
+        }
+        plan.proj_words = words;
+        plan.proj_ready = false;
+        if (words > 0 && words * 8 <= kMaxProjectorBytes) {
+            plan.d_proj.alloc(sizeof(double) * words);
+            upload_vec(plan.d_proj_off, plan.proj_off, s);
+            launch_pair_projectors(plan.d_pair_A.as<int>(), plan.d_pair_B.as<int>(), plan.d_shell_xyz.as<double>(),
+                                   plan.d_shell_L.as<int>(), plan.d_proj_off.as<long long>(), static_cast<int>(np),
+                                   plan.d_proj.as<double>(), s);
+            plan.proj_ready = true;
+        }
+    }
     TLNO_CUDA(cudaStreamSynchronize(s));
 }
 

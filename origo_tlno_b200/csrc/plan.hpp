@@ -11,6 +11,11 @@
 
 namespace tlno_gpu {
 
+// Largest pair-projector table a plan keeps on the device; above it the
+// generic classes run the warp-per-quartet kernel, which builds projectors
+// per quartet.
+constexpr long long kMaxProjectorBytes = 8LL << 30;
+
 struct Tuning {
     int generic_bk = 64;    // ket pairs per tile of the warp-per-quartet kernel
     int generic_warps = 0;  // 0 = from shared-memory budget
@@ -76,6 +81,12 @@ public:
     // Shell-level metric of this plan: false = Schwarz bounds, true = the
     // heuristic decay indicator (integral_threshold must then be 0).
     bool decay_metric = false;
+    // Pair projectors (HRR + spherical maps) of the pair classes the generic
+    // class combinations use: per pair its offset into d_proj or -1.
+    std::vector<long long> proj_off;
+    DeviceBuffer d_proj, d_proj_off;
+    long long proj_words = 0;
+    bool proj_ready = false;
     long long total_quartets = 0, total_prim_quartets = 0;
     double total_flops = 0.0;
     long long total_pairs = 0, kept_pairs = 0;
