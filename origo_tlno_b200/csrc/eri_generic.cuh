@@ -29,6 +29,7 @@ constexpr int kGenericBatch = 32;
 struct GenericLayout {
     int las, lcs;        // La+Lb, Lc+Ld
     int ks, gs;          // k stride (Lc+Ld+1), per-axis G size
+    int gslot;           // doubles per item slot: 3 gs rounded up to odd (conflict-free per-lane slots)
     int nas, ncs;        // radial slice sizes
     int nsab, nscd;      // spherical pair sizes
     int na, nb, nc, nd;  // spherical sizes per shell
@@ -45,7 +46,8 @@ struct GenericLayout {
         na = nsph(la); nb = nsph(lb); nc = nsph(lc); nd = nsph(ld);
         nsab = na * nb;
         nscd = nc * nd;
-        const int g_words = kGenericBatch * 3 * gs;
+        gslot = (3 * gs) | 1;
+        const int g_words = kGenericBatch * gslot;
         off_X = 0;
         off_V = off_X + nas * nscd;
         off_P = off_V + nsab * nscd;
@@ -79,18 +81,20 @@ __device__ __forceinline__ void vrr_2d(R* G, int las, int lcs, int ks, R c00, R 
     }
 }
 
-// Builds the dense (HRR + spherical) projector for one shell pair:
-// Pm[s_ab * nslice + (flat(a') - off(la))] for |a'| in [la, la+lb].
+// Builds the dense (HRR + spherical) projector for one shell pair: element
+// (s_ab, flat(a') - off(la)), |a'| in [la, la+lb], at Pm[s_ab * rs + col * cs]
+// (rs = nslice, cs = 1: row-major; rs = 1, cs = rows: transposed).
 __device__ __forceinline__ void build_pair_projector(double* Pm, int la, int lb,
                                                      double abx, double aby, double abz,
-                                                     int lane) {
+                                                     int lane, bool transposed = false) {
     const int na = nsph(la), nb = nsph(lb);
     const int nslice = ncart_cum(la + lb) - cart_offset(la);
     const int off_a = cart_offset(la), off_b = cart_offset(lb);
+    const int rs = transposed ? 1 : nslice, cs = transposed ? na * nb : 1;
     const double ab[3] = {abx, aby, abz};
     for (int row = lane; row < na * nb; row += 32) {
-        double* out = Pm + row * nslice;
-        for (int c = 0; c < nslice; ++c) out[c] = 0.0;
+        double* out = Pm + row * rs;
+        for (int c = 0; c < nslice; ++c) out[c * cs] = 0.0;
         const int sa = row / nb, sb = row % nb;
         for (int ea = c_c2s.start[la]; ea < c_c2s.start[la] + c_c2s.count[la]; ++ea) {
             if (c_c2s.sph[ea] != sa) continue;
@@ -121,7 +125,7 @@ __device__ __forceinline__ void build_pair_projector(double* Pm, int la, int lb,
                     for (int uy = 0; uy <= bxyz[1]; ++uy)
                         for (int uz = 0; uz <= bxyz[2]; ++uz) {
                             const int col = cart_flat(ax + ux, ay + uy, az + uz) - off_a;
-                            out[col] += kab * fx[ux] * fy[uy] * fz[uz];
+                            out[col * cs] += kab * fx[ux] * fy[uy] * fz[uz];
                         }
             }
         }
@@ -156,7 +160,7 @@ __device__ void generic_quartet(const PlanView& pv, const ClassLaunch& cl,
     const R Ax = R(xa[0]), Ay = R(xa[1]), Az = R(xa[2]);
     const R Cx = R(xc[0]), Cy = R(xc[1]), Cz = R(xc[2]);
     const int n_items = npb * npk * nroots;
-    const int gslot = 3 * lay.gs;
+    const int gslot = lay.gslot;
     const int offa = cart_offset(la), offc = cart_offset(lc);
     // Primitive FASTSCHWARZ (J/K mode, classes up to f as the reference's
     // shell4 portfolio): a dropped primitive quartet gets a zero seed.
@@ -416,7 +420,7 @@ __global__ void eri_generic_jk_kernel(PlanView pv, ClassLaunch cl) {
 // Shared memory (doubles): region0 = max(NB item slots x 3 2-D tables,
 // X + V + the six density blocks), then the radial block T.
 struct GenericCtaLayout {
-    int las, lcs, ks, gs, nas, ncs, na, nb, nc, nd, nsab, nscd;
+    int las, lcs, ks, gs, gslot, nas, ncs, na, nb, nc, nd, nsab, nscd;
     int nb_items;  // item slots per batch
     int off_X, off_V, off_P, off_T, words;
     __host__ __device__ void init(int la, int lb, int lc, int ld, int nbi) {
@@ -430,7 +434,9 @@ struct GenericCtaLayout {
         nsab = na * nb;
         nscd = nc * nd;
         nb_items = nbi;
-        const int g_words = nb_items * 3 * gs;
+        // odd slot size: the threads' own slots fall in different banks
+        gslot = (3 * gs) | 1;
+        const int g_words = nb_items * gslot;
         off_X = 0;
         off_V = off_X + nas * nscd;
         off_P = off_V + nsab * nscd;
@@ -440,7 +446,9 @@ struct GenericCtaLayout {
     }
 };
 
-// Projector block of one shell pair: Pm[s_ab * nslice + (flat(a') - off(la))].
+// Projector block of one shell pair, stored transposed:
+// Pm[(flat(a') - off(la)) * rows + s_ab], rows = (2la+1)(2lb+1), so that the
+// threads of a warp, which take consecutive rows, read consecutive words.
 __device__ __forceinline__ int pair_projector_words(int la, int lb) {
     return nsph(la) * nsph(lb) * (ncart_cum(la + lb) - cart_offset(la));
 }
@@ -456,7 +464,8 @@ __global__ void pair_projector_kernel(const int* pair_A, const int* pair_B, cons
         const int A = pair_A[k], B = pair_B[k];
         const double* xa = shell_xyz + 3 * A;
         const double* xb = shell_xyz + 3 * B;
-        build_pair_projector(out + o, shell_L[A], shell_L[B], xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2], lane);
+        build_pair_projector(out + o, shell_L[A], shell_L[B], xa[0] - xb[0], xa[1] - xb[1], xa[2] - xb[2], lane,
+                             true);
     }
 }
 
@@ -482,7 +491,7 @@ __device__ void generic_quartet_cta(const PlanView& pv, const ClassLaunch& cl, c
     const R Ax = R(xa[0]), Ay = R(xa[1]), Az = R(xa[2]);
     const R Cx = R(xc[0]), Cy = R(xc[1]), Cz = R(xc[2]);
     const int n_items = npb * npk * nroots;
-    const int gslot = 3 * lay.gs;
+    const int gslot = lay.gslot;
     const int offa = cart_offset(la), offc = cart_offset(lc);
     const bool fs_on = cl.fs_thr2 > 0.0 && la <= 3 && lb <= 3 && lc <= 3 && ld <= 3;
     for (int base = 0; base < n_items; base += lay.nb_items) {
@@ -538,26 +547,25 @@ __device__ void generic_quartet_cta(const PlanView& pv, const ClassLaunch& cl, c
         __syncthreads();
     }
 
-    // HRR + spherical projection with the plan's pair projectors:
-    // X = T PK^T, V = PB X.
-    const double* PB = pv.proj + pv.proj_off[bra];
-    const double* PK = pv.proj + pv.proj_off[ket];
+    // HRR + spherical projection with the plan's (transposed) pair
+    // projectors: X = T PK^T, V = PB X.  Consecutive threads take
+    // consecutive ket rows s (coalesced PK reads) and share the bra row.
+    const double* PBt = pv.proj + pv.proj_off[bra];
+    const double* PKt = pv.proj + pv.proj_off[ket];
     double* X = sm + lay.off_X;
     double* V = sm + lay.off_V;
     for (int e = tid; e < lay.nas * lay.nscd; e += nt) {
         const int ia = e / lay.nscd, s = e - ia * lay.nscd;
         const R* trow = T + ia * lay.ncs;
-        const double* prow = PK + s * lay.ncs;
         double acc = 0.0;
-        for (int ic = 0; ic < lay.ncs; ++ic) acc += double(trow[ic]) * __ldg(prow + ic);
+        for (int ic = 0; ic < lay.ncs; ++ic) acc += double(trow[ic]) * __ldg(PKt + ic * lay.nscd + s);
         X[e] = acc;
     }
     __syncthreads();
     for (int e = tid; e < lay.nsab * lay.nscd; e += nt) {
         const int sab = e / lay.nscd, s = e - sab * lay.nscd;
-        const double* prow = PB + sab * lay.nas;
         double acc = 0.0;
-        for (int ia = 0; ia < lay.nas; ++ia) acc += __ldg(prow + ia) * X[ia * lay.nscd + s];
+        for (int ia = 0; ia < lay.nas; ++ia) acc += __ldg(PBt + ia * lay.nsab + sab) * X[ia * lay.nscd + s];
         V[e] = acc;
     }
     __syncthreads();

@@ -40,8 +40,9 @@ struct PlanView {
     const int* mol_shell_off;
     const int* mol_ns;
     // HRR + spherical projector of each pair used by a generic class
-    // combination: proj + proj_off[pair], rows s_ab of ncart slices
-    // |a'| in [La, La+Lb]; null when the plan keeps none.
+    // combination: proj + proj_off[pair], stored transposed (column = the
+    // Cartesian slice |a'| in [La, La+Lb], row = s_ab, rows contiguous);
+    // null when the plan keeps none.
     const double* proj;
     const long long* proj_off;
 };
