@@ -335,7 +335,8 @@ int tlno_gpu_set_combo_generic(tlno_gpu_context* ctx, int combo_id, int force_ge
 int tlno_gpu_plan_combos(const tlno_gpu_context* ctx, int max_n, int* ints, double* dbl);
 /* Per-class tuning of the current plan (the per-class autotuner's knobs;
  * no reference counterpart): the split threshold of class combination
- * combo_index is mixed_threshold x mixed_scale (> 0), and its compile-time
+ * combo_index is mixed_threshold x mixed_scale (>= 0; 0 keeps the class in
+ * FP64 in a mixed build: one launch, no FP32 pass), and its compile-time
  * kernel takes tile_chunk tiles of 32 ket pairs per fetch of its dynamic
  * schedule (1..64; 0 = the kernel's default of 4).  Re-planning resets
  * them.  A captured J/K graph keeps the values of its capture. */

@@ -71,7 +71,9 @@ def tune_mixed_threshold(ctx, D, candidates: Iterable[float] = DEFAULT_CANDIDATE
             "tolerances": {"abs_dE": tol_energy, "max_abs_dJK": tol_jk}}
 
 
-CLASS_CANDIDATES = (1e-1, 1e-2, 1e-3, 1e-4, 1e-5, 1e-6)
+# 0.0 keeps a class in FP64 (one launch, no FP32 pass): the starting point
+# of every class, left only where an FP32 split saves time.
+CLASS_CANDIDATES = (0.0, 1e-1, 1e-2, 1e-3, 1e-4, 1e-5, 1e-6)
 
 
 def _class_jk(ctx, i, D, J, K, mixed):
@@ -96,7 +98,8 @@ def tune_classes(ctx, D, tol_energy: float = 1e-7, tol_jk: float = 1e-8,
     candidate threshold t, in FP64 and mixed (tlno_gpu_class_jk), giving its
     error e_c(t) = (max|dJ_c|, max|dK_c|, |dE_c|) and its kernel time.  J, K
     and E are sums over classes, so sum_c e_c bounds the build's error; a
-    greedy allocation starts every class at the smallest candidate and keeps
+    greedy allocation starts every class at the smallest candidate (0: the
+    class stays FP64, one launch) and keeps
     raising the threshold of the class with the largest time saved per unit
     of budget used while the summed errors stay within the tolerances.  The
     thresholds become per-class multipliers of a unit global threshold.

@@ -228,11 +228,14 @@ void enqueue_jk(Plan2e& plan, const Tuning& tune, const BuildSpec& spec, const d
         cl.want_j = want_j;
         cl.want_k = want_k;
         const int grid = sms * tune.grid_mult;
-        const int passes = mixed ? 2 : 1;
+        // a class whose split multiplier is 0 stays FP64 in a mixed build
+        // (one launch, no FP32 pass)
+        const bool split = mixed && cs.mix_scale > 0.0;
+        const int passes = split ? 2 : 1;
         for (int pass = 0; pass < passes; ++pass) {
-            cl.prec_mode = mixed ? (pass + 1) : 0;
+            cl.prec_mode = split ? (pass + 1) : 0;
             cl.counter = plan.d_counters.as<int>() + 2 * ci + pass;
-            const bool fp32 = mixed && pass == 1;
+            const bool fp32 = split && pass == 1;
             if (cs.fast) {
                 launch_eri_jk_fast(pv, cl, fp32, grid, cs_stream);
             } else {
@@ -970,7 +973,7 @@ int tlno_gpu_set_class_tuning(tlno_gpu_context* ctx, int combo_index, double mix
         if (!ctx || !ctx->plan) throw Error(TLNO_GPU_E_STATE, "tlno_gpu: no plan");
         if (combo_index < 0 || combo_index >= static_cast<int>(ctx->plan->combos.size()))
             throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: combo index out of range");
-        if (!finite_bits(mixed_scale) || !(mixed_scale > 0.0) || tile_chunk < 0 || tile_chunk > 64)
+        if (!finite_bits(mixed_scale) || !(mixed_scale >= 0.0) || tile_chunk < 0 || tile_chunk > 64)
             throw Error(TLNO_GPU_E_INVALID, "tlno_gpu: class tuning value out of range");
         ctx->plan->combos[combo_index].mix_scale = mixed_scale;
         ctx->plan->combos[combo_index].chunk = tile_chunk;
@@ -1028,10 +1031,11 @@ int tlno_gpu_class_jk(tlno_gpu_context* ctx, int combo_index, const double* d_de
         TLNO_CUDA(cudaEventCreate(&e0));
         TLNO_CUDA(cudaEventCreate(&e1));
         TLNO_CUDA(cudaEventRecord(e0, s));
-        for (int pass = 0; pass < (mixed ? 2 : 1); ++pass) {
-            cl.prec_mode = mixed ? pass + 1 : 0;
+        const bool split = mixed && cs.mix_scale > 0.0;
+        for (int pass = 0; pass < (split ? 2 : 1); ++pass) {
+            cl.prec_mode = split ? pass + 1 : 0;
             cl.counter = plan.d_counters.as<int>() + 2 * combo_index + pass;
-            const bool fp32 = mixed && pass == 1;
+            const bool fp32 = split && pass == 1;
             if (cs.fast)
                 launch_eri_jk_fast(pv, cl, fp32, sms * ctx->tune.grid_mult, s);
             else

@@ -259,6 +259,27 @@ def test_per_class_autotuner_cfg1():
     ctx.close()
 
 
+def test_class_scale_zero_keeps_class_fp64():
+    # split multiplier 0: the class runs only its FP64 launch in a mixed
+    # build, so a mixed build with every class at 0 is the FP64 build
+    from origo_tlno_b200 import _native as N
+    mol = M.cfg1()
+    ctx = E.Context(mol).plan(E.ScreeningOptions(integral_threshold=1e-12, mixed_threshold=1e-3))
+    D = M.density_for("cfg1", mol)
+    ref = ctx.jk(D, mixed=False)
+    split = ctx.jk(D, mixed=True)
+    for i in range(len(ctx.combos())):
+        N.check(N.lib().tlno_gpu_set_class_tuning(ctx.h, i, 0.0, 0))
+    out = ctx.jk(D, mixed=True)
+    dJ, dK = _maxabs(out["J"], ref["J"]), _maxabs(out["K"], ref["K"])
+    print(f"PIN class_scale_zero_cfg1 J={dJ:.2e} K={dK:.2e} split_J={_maxabs(split['J'], ref['J']):.2e}")
+    assert dJ < 1e-13 and dK < 1e-13
+    assert _maxabs(split["J"], ref["J"]) > 1e-12  # the split itself is in use at 1e-3
+    with pytest.raises(N.TlnoError):
+        N.check(N.lib().tlno_gpu_set_class_tuning(ctx.h, 0, -1.0, 0))
+    ctx.close()
+
+
 def test_class_launches_over_streams_match_one_stream():
     # the class launches of a build spread over 4 streams (parallel graph
     # branches) give the one-stream result; single context and batch
