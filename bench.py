@@ -431,12 +431,47 @@ def run_batch(args):
 
     nd = args.warmup + args.steps
     out = {}
+    sampler = ClockSampler(local)
     for mixed in (False, True):
         batch.graph_capture(D.data_ptr(), J.data_ptr(), K.data_ptr(), mixed=mixed)
-        ms = timed(batch.graph_launch, batch.stream(), nd)[args.warmup:]
+        if not mixed:
+            with sampler:
+                ms = timed(batch.graph_launch, batch.stream(), nd)[args.warmup:]
+        else:
+            ms = timed(batch.graph_launch, batch.stream(), nd)[args.warmup:]
         out[mixed] = (float(np.sum(ms)) / 1e3, J.clone(), K.clone())
     t64, J64, K64 = out[False]
     tmx, Jmx, Kmx = out[True]
+    # end to end through the host-buffer batch call (H2D of the stacked
+    # densities, D2H of J and K), FP64
+    Dh = [d.numpy() for d in Ds]
+    e2e_t = []
+    for _ in range(3):
+        t0 = time.time()
+        Jh, Kh = batch.jk(Dh, mixed=False)
+        e2e_t.append(time.time() - t0)
+    e2e_s = float(np.median(e2e_t[1:]))
+    # reference CPU engine on a bounded sample: the first molecules of the
+    # batch, one J+K build each, one core
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+            secs = 0.0
+            qs = 0
+            n = 0
+            for i, m in enumerate(mols):
+                if secs > 10.0:
+                    break
+                rb = ref.RefBasis(m)
+                secs += float(rb.time_jk(Ds[i].numpy(), schwarz=1e-12, reps=1)[0])
+                qs += _count_quartets(m, 1e-12)
+                n += 1
+            cpu = {"value": qs / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"the first {n} molecules of the batch, one J+K build each ({qs} quartets, {secs:.2f} s)",
+                   "host": _host_cpu(), "route": ROUTES[ref.ROUTE]}
+        except Exception as e:  # the reference oracle may be absent
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
     # one context (and one graph) per molecule, back to back
     seq = 0.0
     for i, c in enumerate(ctxs):
@@ -447,20 +482,31 @@ def run_batch(args):
         c.graph_capture(Di.data_ptr(), Ji.data_ptr(), Ki.data_ptr(), mixed=False)
         seq += min(timed(c.graph_launch, c.stream(), 2)) / 1e3
     q = prof["quartets"]
-    res = {"metric": METRIC, "value": q * args.steps / tmx, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1e3 * tmx / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 mixed (FP64 accumulation)",
+    # The batch has no per-class split tuning: at the safe fixed split the
+    # mixed build is not faster here, so the headline is the FP64 batch and
+    # the mixed one is reported beside it.
+    res = {"metric": METRIC, "value": q * args.steps / t64, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * t64 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
            "config": {"workload": "cfg3", "description": "256 molecules of 3-30 atoms in one batch, Schwarz 1e-12",
                       "l2": "L2 flushed between timed builds (256 MB write)",
                       "molecules": len(mols), "functions_total": prof["M"], "quartets_per_build": q,
-                      "streams": args.streams,
-                      "mixed_threshold": args.mixed_threshold},
-           "fp64": {"value": q * args.steps / t64, "unit": UNIT, "ms_per_step": 1e3 * t64 / args.steps},
+                      "streams": args.streams},
+           "mixed": {"value": q * args.steps / tmx, "unit": UNIT, "ms_per_step": 1e3 * tmx / args.steps,
+                     "mixed_threshold": args.mixed_threshold,
+                     "accuracy": {"max_abs_dJ": float((Jmx - J64).abs().max()),
+                                  "max_abs_dK": float((Kmx - K64).abs().max())}},
            "one_context_per_molecule_fp64_ms": 1e3 * seq,
            "batched_speedup_vs_one_context_per_molecule": seq / (t64 / args.steps),
-           "accuracy": {"max_abs_dJ": float((Jmx - J64).abs().max()), "max_abs_dK": float((Kmx - K64).abs().max())},
-           "gpu_launches": None}
+           "e2e": {"value": q / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(sum(d.nbytes for d in Dh)),
+                   "d2h_bytes_per_step": int(sum(a.nbytes for a in Jh) + sum(a.nbytes for a in Kh))},
+           # per build: one launch per class combination over all molecules
+           # and the two symmetrisations
+           "gpu_launches": (prof["n_class_launches"] + 2) * args.steps,
+           "roofline": None,
+           "clocks": sampler.summary(),
+           "cpu_baseline": cpu}
     if rank == 0:
         print(json.dumps(res))
     return 0
