@@ -11,7 +11,7 @@
 // contracted radial integrals (a0|c0): rows ia = g, g+TPQ, ... of the
 // NAS x NCS block, g = warp index inside the group.  The slice is fixed at
 // compile time, so the accumulators stay in registers; TPQ is the smallest
-// power of two whose slice holds at most kMaxAccPerSlice accumulators.
+// power of two whose slice holds at most fast_acc_limit() accumulators.
 // Phase 2: ket HRR and ket spherical projection of the owned rows, written
 // to shared memory as (a0|cd)_sph rows.
 // Phase 3: after a barrier, each warp takes a share of the ket columns
@@ -76,14 +76,23 @@ __host__ __device__ constexpr bool c2s_nz(int L, int s, int c) {
     return true;
 }
 
-constexpr int kMaxAccPerSlice = 64;
 constexpr int kTileChunk = 4;  // default tiles per dynamic-schedule fetch
 constexpr int kBraGroup = 8;   // bras per block of the light classes
 constexpr int kMaxCarried = 24;
 
-__host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs) {
+// Radial accumulators per thread slice.  Every slice of a quartet repeats the
+// primitive loop (roots, 2-D VRR) and is its own unrolled copy of the code,
+// so fewer, wider slices win although they need more registers: d classes
+// 128 (cfg4 (dp|pp): FP64 1108 -> 757 ms, FP32 934 -> 579 ms, with FP64
+// spills), except (dp|dp), which spills too much in FP64 (310 -> 391 ms) and
+// keeps 64; the f classes keep 64.
+__host__ __device__ constexpr int fast_acc_limit(int la, int lb, int lc, int ld) {
+    return (la <= 2 && lb <= 2 && lc <= 2 && ld <= 2 && !(la == 2 && lb == 1 && lc == 2 && ld == 1)) ? 128 : 64;
+}
+
+__host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs, int acc) {
     int t = 1;
-    while (t < 32 && ((nas + t - 1) / t) * ncs > kMaxAccPerSlice) t *= 2;
+    while (t < 32 && ((nas + t - 1) / t) * ncs > acc) t *= 2;
     return t;
 }
 
@@ -100,7 +109,7 @@ struct FastShape {
     static constexpr int NSA = ce_nsph(LA), NSB = ce_nsph(LB);
     static constexpr int NSC = ce_nsph(LC), NSD = ce_nsph(LD);
     static constexpr int NSAB = NSA * NSB, NSCD = NSC * NSD;
-    static constexpr int TPQ = fast_pick_tpq(NAS, NCS);
+    static constexpr int TPQ = fast_pick_tpq(NAS, NCS, fast_acc_limit(LA, LB, LC, LD));
     static constexpr int BBQ = TPQ >= 4 ? 1 : 4 / TPQ;
     static constexpr int WARPS = TPQ * BBQ;
     // Phase-3 work split: by ket spherical function c when there are enough
@@ -373,11 +382,15 @@ __device__ __forceinline__ bool group_any(bool pred, int id, int nthreads) {
 // The lightest classes (at most 9 radial accumulators per thread) are
 // latency-bound on their gathers: a register cap of 4 resident CTAs per SM
 // (FP64) or 6 (FP32) buys more warps than it costs (measured on 200 waters);
-// classes with larger accumulator blocks would spill under it.
+// classes with larger accumulator blocks would spill under it.  FP32 (ps|ss)
+// takes 7 (cfg4: 1199 -> 1119 ms; 7 or 8 is slower or equal on the other
+// light classes).
 template <typename R, int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr int fast_min_blocks() {
     using S = FastShape<LA, LB, LC, LD>;
-    return (S::TPQ == 1 && S::NAS * S::NCS <= 9) ? (std::is_same<R, float>::value ? 6 : 4) : 1;
+    if (!(S::TPQ == 1 && S::NAS * S::NCS <= 9)) return 1;
+    if (!std::is_same<R, float>::value) return 4;
+    return (LA == 1 && LB == 0 && LC == 0 && LD == 0) ? 7 : 6;
 }
 
 // Where a bra-group class keeps the per-tile density values of a lane:
