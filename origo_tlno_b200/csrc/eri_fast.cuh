@@ -82,12 +82,12 @@ constexpr int kMaxCarried = 24;
 
 // Radial accumulators per thread slice.  Every slice of a quartet repeats the
 // primitive loop (roots, 2-D VRR) and is its own unrolled copy of the code,
-// so fewer, wider slices win although they need more registers: d classes
-// 128 (cfg4 (dp|pp): FP64 1108 -> 757 ms, FP32 934 -> 579 ms, with FP64
-// spills), except (dp|dp), which spills too much in FP64 (310 -> 391 ms) and
-// keeps 64; the f classes keep 64.
+// so fewer, wider slices win although they need more registers: 128
+// (cfg4 (dp|pp): FP64 1108 -> 757 ms, FP32 934 -> 579 ms, with FP64 spills;
+// cfg2's compile-time f classes: FP64 1639 -> 1126 ms, FP32 1474 -> 783 ms),
+// except (dp|dp), which spills too much in FP64 (310 -> 391 ms) and keeps 64.
 __host__ __device__ constexpr int fast_acc_limit(int la, int lb, int lc, int ld) {
-    return (la <= 2 && lb <= 2 && lc <= 2 && ld <= 2 && !(la == 2 && lb == 1 && lc == 2 && ld == 1)) ? 128 : 64;
+    return (la == 2 && lb == 1 && lc == 2 && ld == 1) ? 64 : 128;
 }
 
 __host__ __device__ constexpr int fast_pick_tpq(int nas, int ncs, int acc) {
