@@ -330,7 +330,7 @@ def test_cfg2_full_molecule_against_reference_fixture():
                           dE=abs((np.sum(D * J) - 0.5 * np.sum(D * K)) - (g["trDJ"] - 0.5 * g["trDK"])))
     _record("cfg2_full_fp64", **{k: float(v) for k, v in res[False].items()})
     _record("cfg2_full_mixed_1e-5", **{k: float(v) for k, v in res[True].items()})
-    assert max(res[False]["sJ"], res[False]["sK"]) < 5e-12
-    assert res[False]["dE"] < 1e-9
+    assert max(res[False]["sJ"], res[False]["sK"]) < 1e-12
+    assert res[False]["dE"] < 1e-10
     assert max(res[True]["sJ"], res[True]["sK"]) < 1e-7 and res[True]["dE"] < 1e-6
     ctx.close()
