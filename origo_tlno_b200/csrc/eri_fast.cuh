@@ -388,10 +388,17 @@ __device__ __forceinline__ bool group_any(bool pred, int id, int nthreads) {
 template <typename R, int LA, int LB, int LC, int LD>
 __host__ __device__ constexpr int fast_min_blocks() {
     using S = FastShape<LA, LB, LC, LD>;
-    // unsliced FP32 classes with larger accumulator blocks ((pp|ps), (ds|ps),
-    // (dp|ps), ...): 3 resident CTAs instead of the 2 their ~200 registers
-    // allow
-    if (S::TPQ == 1 && S::NAS * S::NCS > 9) return std::is_same<R, float>::value ? 3 : 1;
+    // unsliced FP32 classes with larger accumulator blocks: 3 resident CTAs
+    // instead of the 2 their ~200 registers allow, 4 for (pp|ps), (ds|ps),
+    // (dp|ss), (ds|ds), (dd|ss) (measured per class on 200 waters; 4 is
+    // slower on the others)
+    if (S::TPQ == 1 && S::NAS * S::NCS > 9) {
+        if (!std::is_same<R, float>::value) return 1;
+        constexpr bool four = (LA == 1 && LB == 1 && LC == 1 && LD == 0) || (LA == 2 && LB == 0 && LC == 1 && LD == 0) ||
+                              (LA == 2 && LB == 1 && LC == 0 && LD == 0) || (LA == 2 && LB == 0 && LC == 2 && LD == 0) ||
+                              (LA == 2 && LB == 2 && LC == 0 && LD == 0);
+        return four ? 4 : 3;
+    }
     if (!(S::TPQ == 1 && S::NAS * S::NCS <= 9)) return 1;
     if (!std::is_same<R, float>::value) return 4;
     return (LA == 1 && LB == 0 && LC == 0 && LD == 0) ? 7 : 6;
