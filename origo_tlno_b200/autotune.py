@@ -90,6 +90,42 @@ def _set_class(ctx, i, scale, chunk):
     N.check(N.lib().tlno_gpu_set_class_tuning(ctx.h, i, scale, chunk))
 
 
+def allocate_budget(rows, tol_energy: float, tol_jk: float):
+    """Greedy allocation of the accuracy budget over classes.
+
+    `rows`: per class {"trials": [{"ms", "max_abs_dJ", "max_abs_dK",
+    "abs_dE"}, ...] ordered by increasing split threshold, "pick": index}.
+    Every class starts at its pick (the first trial: the class in FP64);
+    the step with the largest time saved per unit of budget used is taken
+    while the summed per-class errors stay within the tolerances.  Sets each
+    row's "pick" and returns the summed (max|dJ|, max|dK|, |dE|)."""
+    def used(r, k):
+        tr = r["trials"][k]
+        return tr["max_abs_dJ"], tr["max_abs_dK"], tr["abs_dE"]
+    sJ = sum(used(r, r["pick"])[0] for r in rows)
+    sK = sum(used(r, r["pick"])[1] for r in rows)
+    sE = sum(used(r, r["pick"])[2] for r in rows)
+    while True:
+        best = None
+        for r in rows:
+            k = r["pick"]
+            for k2 in range(k + 1, len(r["trials"])):
+                a, b = used(r, k), used(r, k2)
+                nJ, nK, nE = sJ - a[0] + b[0], sK - a[1] + b[1], sE - a[2] + b[2]
+                if nJ > tol_jk or nK > tol_jk or nE > tol_energy:
+                    break
+                gain = r["trials"][k]["ms"] - r["trials"][k2]["ms"]
+                cost = max((b[0] - a[0]) / tol_jk, (b[1] - a[1]) / tol_jk, (b[2] - a[2]) / tol_energy, 1e-12)
+                score = gain / cost
+                if gain > 0 and (best is None or score > best[0]):
+                    best = (score, r, k2, nJ, nK, nE)
+        if best is None:
+            break
+        _, r, k2, sJ, sK, sE = best
+        r["pick"] = k2
+    return sJ, sK, sE
+
+
 def tune_classes(ctx, D, tol_energy: float = 1e-7, tol_jk: float = 1e-8,
                  candidates: Iterable[float] = CLASS_CANDIDATES, chunks: Iterable[int] = ()) -> dict:
     """Per-class autotuner of the mixed path on the device density `D`.
@@ -139,31 +175,7 @@ def tune_classes(ctx, D, tol_energy: float = 1e-7, tol_jk: float = 1e-8,
             trials.append({"threshold": t, "ms": ms, "max_abs_dJ": dJ, "max_abs_dK": dK, "abs_dE": dE})
         rows.append({"index": i, "class": f"{combos[i]['la']}{combos[i]['lb']}|{combos[i]['lc']}{combos[i]['ld']}",
                      "chunk": chunk, "fp64_ms": t64, "trials": trials, "pick": 0})
-    # greedy allocation of the error budget
-    def used(r, k):
-        tr = r["trials"][k]
-        return tr["max_abs_dJ"], tr["max_abs_dK"], tr["abs_dE"]
-    sJ = sum(used(r, 0)[0] for r in rows)
-    sK = sum(used(r, 0)[1] for r in rows)
-    sE = sum(used(r, 0)[2] for r in rows)
-    while True:
-        best = None
-        for r in rows:
-            k = r["pick"]
-            for k2 in range(k + 1, len(cands)):
-                a, b = used(r, k), used(r, k2)
-                nJ, nK, nE = sJ - a[0] + b[0], sK - a[1] + b[1], sE - a[2] + b[2]
-                if nJ > tol_jk or nK > tol_jk or nE > tol_energy:
-                    break
-                gain = r["trials"][k]["ms"] - r["trials"][k2]["ms"]
-                cost = max((b[0] - a[0]) / tol_jk, (b[1] - a[1]) / tol_jk, (b[2] - a[2]) / tol_energy, 1e-12)
-                score = gain / cost
-                if gain > 0 and (best is None or score > best[0]):
-                    best = (score, r, k2, nJ, nK, nE)
-        if best is None:
-            break
-        _, r, k2, sJ, sK, sE = best
-        r["pick"] = k2
+    sJ, sK, sE = allocate_budget(rows, tol_energy, tol_jk)
     total = 0.0
     for r in rows:
         tr = r["trials"][r["pick"]]

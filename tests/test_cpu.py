@@ -371,3 +371,32 @@ def test_frontend_named_basis_matches_build_basis_general(name, basis):
     assert np.array_equal(a, a_ref) and np.array_equal(n, n_ref)
     assert np.array_equal(c, c_ref) and np.array_equal(e, e_ref)
     assert np.max(np.abs(k - k_ref) / np.abs(k_ref)) < 1e-14
+
+
+def _trials(ms, err):
+    return [{"ms": m, "max_abs_dJ": e, "max_abs_dK": e, "abs_dE": e} for m, e in zip(ms, err)]
+
+
+def test_budget_allocation_keeps_unprofitable_classes_fp64():
+    # per-class split allocation of the mixed path: a class whose FP32 split
+    # saves no time stays at its first trial (FP64 only, one launch); the
+    # summed per-class errors stay inside the tolerances
+    from origo_tlno_b200.autotune import allocate_budget
+    rows = [
+        {"trials": _trials([10.0, 8.0, 6.0, 5.0], [0.0, 1e-9, 1e-8, 1e-7]), "pick": 0},  # profitable
+        {"trials": _trials([4.0, 4.2, 4.5, 5.0], [0.0, 1e-10, 1e-9, 1e-8]), "pick": 0},  # FP32 slower
+        {"trials": _trials([7.0, 5.0, 4.0, 3.0], [0.0, 5e-9, 2e-8, 9e-8]), "pick": 0},   # profitable
+    ]
+    sJ, sK, sE = allocate_budget(rows, tol_energy=1e-7, tol_jk=3e-8)
+    assert rows[1]["pick"] == 0
+    assert rows[0]["pick"] > 0 and rows[2]["pick"] > 0
+    assert sJ <= 3e-8 and sK <= 3e-8 and sE <= 1e-7
+    picked = sum(r["trials"][r["pick"]]["max_abs_dJ"] for r in rows)
+    assert abs(picked - sJ) < 1e-20
+
+
+def test_budget_allocation_without_budget_keeps_everything_fp64():
+    from origo_tlno_b200.autotune import allocate_budget
+    rows = [{"trials": _trials([10.0, 5.0], [0.0, 1e-6]), "pick": 0} for _ in range(3)]
+    sJ, sK, sE = allocate_budget(rows, tol_energy=1e-7, tol_jk=1e-8)
+    assert all(r["pick"] == 0 for r in rows) and sJ == sK == sE == 0.0
